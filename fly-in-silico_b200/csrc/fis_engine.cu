@@ -1,0 +1,549 @@
+// The fused LIF engine for sm_100a.
+//
+// What one block of K steps (K <= the axonal lag L = buf_len + 1 = 20) does:
+//
+//   phase A  k_scatter   the spikes of steps t0-L .. t0+K-1-L reach the
+//                        conductance exactly at steps t0 .. t0+K-1 (written
+//                        into the reference's ring one step after the spike,
+//                        read buf_len steps later; sim.py:887-897).  Their CSR
+//                        rows are pushed into a scratch ring of K int32 slots
+//                        with integer atomics, a warp per (spike, chunk of
+//                        the row).  Integer sums make the order irrelevant.
+//   phase B  k_update    every neuron of every trial advances K steps with
+//                        its state in registers: refractory counter and gate,
+//                        delayed input, conductance, Poisson drive (Philox),
+//                        membrane, hold, threshold, reset (sim.py:921-952).
+//                        Nothing inside a block depends on a spike of the same
+//                        block, because a spike needs L steps to arrive; so
+//                        the dense state is read and written once per K steps
+//                        instead of once per step.
+//
+// The reference applies m_out to the spikes of step u at step u+1
+// (sim.py:910-913).  Inside a block that mask is the block's own; for the last
+// step of a block it is the next block's, so the last list is written
+// unfiltered and phase A of the next block filters it.
+//
+// Floating point follows the reference's operation order one rounding at a
+// time (__f*_rn intrinsics, never contracted into FMA): the result is the same
+// bits as the reference's float32 torch arithmetic.
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "fis_common.cuh"
+
+namespace fis {
+namespace {
+
+constexpr int kUpdThreads = 256;
+constexpr int kScatThreads = 256;
+constexpr int kScatWarps = kScatThreads / kWarp;
+constexpr int kMaxLists = 11264;  // prefix entries in dynamic shared memory (44 KB)
+
+int sm_count() {
+  static int cached[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return 148;
+  if (!cached[dev]) {
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
+      v = 148;
+    cached[dev] = v;
+  }
+  return cached[dev];
+}
+
+// ---------------------------------------------------------------------------
+// phase A: scatter spike lists into the scratch ring
+// ---------------------------------------------------------------------------
+
+// Source list kk (0 <= kk < nsrc) holds the spikes of step u = u_first + kk;
+// its rows go to ring slot kk, or (slot_mode 1) to the slot of the reference's
+// delay ring that holds the input of step u + lag, which is (u + 1) % buf_len.  With `filter_last`, the
+// list of step t0-1 (the last one written by the previous block) is checked
+// against m_out: when it is also a source, its dead entries are skipped; when
+// it is not (K < L), its dead entries are marked for the block that will
+// consume it.
+struct ScatterArgs {
+  int b0, nb;
+  int nsrc;
+  int64_t u_off;      // u_first = clock + u_off
+  int slot_mode;      // 0: slot kk; 1: the reference ring slot (u + 1) % buf_len
+  int zero_next;      // zero list_len of steps clock .. clock+zero_next-1
+  int filter_last;    // handle the list of step clock-1 as described above
+  int32_t* ring;      // slot stride nb*n, trial stride n
+};
+
+__global__ void __launch_bounds__(kScatThreads)
+k_scatter(const fis_engine E, const ScatterArgs A) {
+  extern __shared__ int32_t pre_sum[];
+  const int n = E.n;
+  const int B = E.batch;
+  const int L = E.p.lag;
+  const int64_t t0 = *E.clock;
+  const int64_t u_first = t0 + A.u_off;
+  const int64_t u_last = t0 - 1;
+  // Is the list of step t0-1 one of the sources?
+  const int kk_last = (int)(u_last - u_first);
+  const bool last_is_src = A.filter_last && kk_last >= 0 && kk_last < A.nsrc;
+  const bool extra = A.filter_last && !last_is_src && u_last >= 0;
+  const int nlists = (A.nsrc + (extra ? 1 : 0)) * A.nb;
+
+  // Prefix sum of the list lengths: entries [j*..] of list j, j = kk*nb + bl.
+  {
+    const int per = (nlists + kScatThreads - 1) / kScatThreads;
+    const int j0 = threadIdx.x * per;
+    int32_t acc = 0;
+    for (int j = j0; j < j0 + per && j < nlists; ++j) {
+      const int kk = j / A.nb, bl = j - kk * A.nb;
+      const int64_t u = (kk < A.nsrc) ? u_first + kk : u_last;
+      int32_t len = 0;
+      if (u >= 0) len = E.list_len[mod_pos(u, 2 * L) * B + A.b0 + bl];
+      pre_sum[j] = len;  // provisional
+      acc += len;
+    }
+    __shared__ int32_t part[kScatThreads];
+    part[threadIdx.x] = acc;
+    __syncthreads();
+    // inclusive scan of the per-thread partial sums (Hillis-Steele)
+    for (int off = 1; off < kScatThreads; off <<= 1) {
+      const int32_t x = threadIdx.x >= off ? part[threadIdx.x - off] : 0;
+      __syncthreads();
+      part[threadIdx.x] += x;
+      __syncthreads();
+    }
+    int32_t run = threadIdx.x ? part[threadIdx.x - 1] : 0;
+    for (int j = j0; j < j0 + per && j < nlists; ++j) {
+      const int32_t len = pre_sum[j];
+      pre_sum[j] = run;
+      run += len;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) pre_sum[nlists] = part[kScatThreads - 1];
+    __syncthreads();
+  }
+  const int32_t total = pre_sum[nlists];
+
+  // Lists that the following update phase will write start empty.
+  if (blockIdx.x == 0) {
+    for (int j = threadIdx.x; j < A.zero_next * A.nb; j += blockDim.x) {
+      const int kk = j / A.nb, bl = j - kk * A.nb;
+      E.list_len[mod_pos(t0 + kk, 2 * L) * B + A.b0 + bl] = 0;
+    }
+  }
+
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int warp = threadIdx.x / kWarp;
+  const int64_t slot_stride = (int64_t)A.nb * n;
+  for (int32_t w = blockIdx.x * kScatWarps + warp; w < total; w += gridDim.x * kScatWarps) {
+    // list holding work item w: largest j with pre_sum[j] <= w
+    int lo = 0, hi = nlists - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (pre_sum[mid] <= w) lo = mid; else hi = mid - 1;
+    }
+    const int j = lo;
+    const int kk = j / A.nb, bl = j - kk * A.nb;
+    const int b = A.b0 + bl;
+    const bool is_src = kk < A.nsrc;
+    const int64_t u = is_src ? u_first + kk : u_last;
+    uint32_t* lst = E.lists + ((int64_t)mod_pos(u, L) * B + b) * E.list_cap;
+    const int32_t idx = w - pre_sum[j];
+    if (idx >= E.list_cap) continue;
+    const uint32_t e = lst[idx];
+    const uint32_t pre = entry_pre(e);
+    if (e == kDeadEntry || pre >= (uint32_t)n) continue;
+    if (A.filter_last && u == u_last) {
+      const uint8_t fl = E.flags[(int64_t)b * n + pre];
+      if (fl & (FIS_FL_OUT_OFF | FIS_FL_SILENCED)) {
+        if (!is_src && lane == 0) lst[idx] = kDeadEntry;
+        continue;
+      }
+    }
+    if (!is_src) continue;
+    const int64_t r0 = E.row_ptr[pre], r1 = E.row_ptr[pre + 1];
+    const int64_t lo_e = r0 + (int64_t)entry_chunk(e) * E.chunk;
+    const int64_t hi_e = min(r1, lo_e + (int64_t)E.chunk);
+    if (lo_e >= hi_e) continue;
+    const int slot = A.slot_mode ? (int)mod_pos(u + 1, E.p.buf_len) : kk;
+    int32_t* dst = A.ring + slot * slot_stride + (int64_t)bl * n;
+    // 16-byte vector loads: four edges per lane, 128 edges per warp pass.
+    for (int64_t p = (lo_e & ~(int64_t)3) + 4 * lane; p < hi_e; p += 4 * kWarp) {
+      const uint4 q = __ldg(reinterpret_cast<const uint4*>(E.edges + p));
+      const uint32_t wv[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int64_t pe = p + c;
+        if (pe >= lo_e && pe < hi_e) {
+          const int post = edge_post(wv[c]);
+          if (post < n) atomicAdd(dst + post, edge_count(wv[c]));
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// phase B: K fused steps per neuron
+// ---------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(kUpdThreads)
+k_update(const fis_engine E, const int b0, const int nb, const int K,
+         int32_t* __restrict__ ring, float* __restrict__ spikes_out,
+         const int bump) {
+  const int n = E.n;
+  const int B = E.batch;
+  const int L = E.p.lag;
+  const int Wd = (n + kWarp - 1) / kWarp;
+  const int64_t npad = (int64_t)Wd * kWarp;
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t t0 = *E.clock;
+
+  if (gid < (int64_t)nb * npad) {
+    const int bl = (int)(gid / npad);
+    const int i = (int)(gid - (int64_t)bl * npad);
+    const int b = b0 + bl;
+    const int word = i >> 5;
+    const int lane = threadIdx.x & (kWarp - 1);
+    const bool valid = i < n;
+    const fis_trial tr = E.trials[b];
+    int64_t ka64 = tr.start - t0, kb64 = tr.end - t0;
+    const int ka = (int)max((int64_t)0, min(ka64, (int64_t)K));
+    const int kb = (int)max((int64_t)0, min(kb64, (int64_t)K));
+
+    // Delayed input of all K steps, loaded up front; consumed slots return to
+    // zero so the scratch ring needs no separate clearing pass.
+    int32_t c[FIS_MAX_BLOCK];
+    const int64_t sstride = (int64_t)nb * n;
+    int32_t* rp = ring + (int64_t)bl * n + i;
+#pragma unroll
+    for (int k = 0; k < FIS_MAX_BLOCK; ++k) {
+      c[k] = 0;
+      if (k < K && valid) c[k] = rp[k * sstride];
+    }
+#pragma unroll
+    for (int k = 0; k < FIS_MAX_BLOCK; ++k)
+      if (k < K && valid && c[k] != 0) rp[k * sstride] = 0;
+
+    const int64_t sidx = (int64_t)b * n + i;
+    float v = 0.f, g = 0.f, r = 0.f, rate = 0.f;
+    uint32_t fl = 0;
+    if (valid && ka < kb) {
+      v = E.v[sidx];
+      g = E.g[sidx];
+      r = E.refrac[sidx];
+      fl = E.flags[sidx];
+      rate = E.rates[sidx];
+    }
+    bool s_prev = false;
+    if (t0 - 1 >= tr.start && t0 >= 1) {
+      const uint32_t wv = E.bits[(mod_pos(t0 - 1, L) * B + b) * Wd + word];
+      s_prev = (wv >> lane) & 1u;
+    }
+    const float m_fire = (fl & FIS_FL_FIRE_OFF) ? 0.f : 1.f;
+    const bool out_on = !(fl & (FIS_FL_OUT_OFF | FIS_FL_SILENCED));
+    const bool silenced = fl & FIS_FL_SILENCED;
+    const float m_in = (fl & FIS_FL_IN_OFF) ? 0.f : 1.f;
+    const bool hold = fl & FIS_FL_HOLD;
+    const float m_hold = hold ? 0.f : 1.f;
+    const float v_hold = hold ? tr.v_clamp : 0.f;
+    const float rs = (fl & FIS_FL_NOREFRAC) ? 0.f : E.p.refrac_steps;
+    const float prob = __fmul_rn(rate, E.p.prob_scale);
+    const bool driven = prob > 0.f;
+    const uint32_t key0 = (uint32_t)tr.seed, key1 = (uint32_t)(tr.seed >> 32);
+
+#pragma unroll
+    for (int k = 0; k < FIS_MAX_BLOCK; ++k) {
+      if (k < K) {
+        const int64_t u = t0 + k;
+        bool fired = false;
+        if (valid && k >= ka && k < kb) {
+          // refractory counter and gate (sim.py:921-923)
+          const float s = s_prev ? 1.f : 0.f;
+          r = __fmul_rn(__fadd_rn(r, 1.f), __fsub_rn(1.f, s));
+          const float gate = (r >= rs) ? 1.f : 0.f;
+          // delayed input and the new conductance (sim.py:928-929)
+          const int32_t ck = silenced ? 0 : c[k];
+          const float delayed = __fmul_rn(__fmul_rn(E.p.w_scale, __int2float_rn(ck)), m_in);
+          const float gn = __fadd_rn(__fmul_rn(g, E.p.a_syn), __fmul_rn(delayed, gate));
+          // Poisson drive (sim.py:859-861): one Philox word per draw
+          float vstim = 0.f;
+          if (E.vstim) {
+            vstim = E.vstim[sidx];
+          } else if (driven) {
+            const int64_t own = u - tr.start;
+            const uint32_t x = philox_x0((uint32_t)i, (uint32_t)own,
+                                         (uint32_t)((uint64_t)own >> 32), tr.stream,
+                                         key0, key1);
+            if (__fmul_rn((float)(x >> 8), 0x1p-24f) < prob) vstim = E.p.kick;
+          }
+          // membrane with the previous conductance (sim.py:936-938)
+          v = __fadd_rn(v, vstim);
+          v = __fadd_rn(v, __fmul_rn(E.p.a_mem, __fsub_rn(g, __fsub_rn(v, E.p.v_rest))));
+          // hold, threshold, reset (sim.py:943-952)
+          v = __fadd_rn(__fmul_rn(v, m_hold), v_hold);
+          const float sp = __fmul_rn((v > E.p.v_th) ? 1.f : 0.f, m_fire);
+          v = __fsub_rn(v, __fmul_rn(__fsub_rn(v, E.p.v_reset), sp));
+          g = __fsub_rn(gn, __fmul_rn(gn, sp));
+          fired = sp != 0.f;
+          s_prev = fired;
+        }
+        const unsigned bal = __ballot_sync(0xFFFFFFFFu, fired);
+        if (lane == 0) E.bits[(mod_pos(u, L) * B + b) * Wd + word] = bal;
+        if (fired) {
+          const int nch = E.nchunks[i];
+          if ((out_on || k == K - 1) && nch > 0) {
+            int32_t* lenp = E.list_len + mod_pos(u, 2 * L) * B + b;
+            const int32_t pos = atomicAdd(lenp, nch);
+            uint32_t* dst = E.lists + ((int64_t)mod_pos(u, L) * B + b) * E.list_cap;
+            for (int q = 0; q < nch; ++q)
+              if (pos + q < E.list_cap) dst[pos + q] = ((uint32_t)i << 8) | (uint32_t)q;
+          }
+          if (tr.rec >= 0 && tr.rec < E.n_recs && tr.bin_steps > 0) {
+            const int64_t bin = (u - tr.start) / tr.bin_steps;
+            if (bin < tr.n_bins) atomicAdd(E.recs[tr.rec] + bin * n + i, 1);
+          }
+        }
+      }
+    }
+    if (valid && ka < kb) {
+      E.v[sidx] = v;
+      E.g[sidx] = g;
+      E.refrac[sidx] = r;
+    }
+    if (spikes_out && valid) spikes_out[sidx] = s_prev ? 1.f : 0.f;
+  }
+
+  if (bump) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      const unsigned prev = atomicAdd(E.done, 1u);
+      if (prev == gridDim.x - 1) {
+        *E.done = 0u;
+        *E.clock = t0 + K;
+        __threadfence();
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------
+
+// scratch [buf_len][nb][n] int32 -> out [nb][buf_len][n] float, w_scale * count
+__global__ void k_ring_to_f32(const fis_engine E, int b0, int nb,
+                              const int32_t* __restrict__ scratch,
+                              float* __restrict__ out) {
+  const int n = E.n, R = E.p.buf_len;
+  const int64_t total = (int64_t)nb * R * n;
+  for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < total;
+       x += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(x % n);
+    const int64_t rest = x / n;
+    const int s = (int)(rest % R);
+    const int bl = (int)(rest / R);
+    const uint8_t fl = E.flags[(int64_t)(b0 + bl) * n + i];
+    const int32_t cnt = (fl & FIS_FL_SILENCED) ? 0 : scratch[((int64_t)s * nb + bl) * n + i];
+    out[x] = __fmul_rn(E.p.w_scale, __int2float_rn(cnt));
+  }
+}
+
+__global__ void k_spikes_f32(const fis_engine E, int b0, int nb, int64_t step,
+                             float* __restrict__ out) {
+  const int n = E.n, B = E.batch, L = E.p.lag;
+  const int Wd = (n + kWarp - 1) / kWarp;
+  const int64_t total = (int64_t)nb * n;
+  for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < total;
+       x += (int64_t)gridDim.x * blockDim.x) {
+    const int bl = (int)(x / n), i = (int)(x % n);
+    const uint32_t wv = E.bits[(mod_pos(step, L) * B + b0 + bl) * Wd + (i >> 5)];
+    out[x] = ((wv >> (i & 31)) & 1u) ? 1.f : 0.f;
+  }
+}
+
+__global__ void k_load_spikes(const fis_engine E, int b0, int nb,
+                              const float* __restrict__ sp) {
+  const int n = E.n, B = E.batch, L = E.p.lag;
+  const int Wd = (n + kWarp - 1) / kWarp;
+  const int64_t u = *E.clock - 1;
+  const int64_t npad = (int64_t)Wd * kWarp;
+  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (u < 0 || gid >= (int64_t)nb * npad) return;
+  const int bl = (int)(gid / npad);
+  const int i = (int)(gid - (int64_t)bl * npad);
+  const int b = b0 + bl;
+  const bool fired = i < n && sp[(int64_t)bl * n + i] != 0.f;
+  const unsigned bal = __ballot_sync(0xFFFFFFFFu, fired);
+  if ((threadIdx.x & 31) == 0) E.bits[(mod_pos(u, L) * B + b) * Wd + (i >> 5)] = bal;
+  if (fired) {
+    const int nch = E.nchunks[i];
+    if (nch > 0) {
+      const int32_t pos = atomicAdd(E.list_len + mod_pos(u, 2 * L) * B + b, nch);
+      uint32_t* dst = E.lists + ((int64_t)mod_pos(u, L) * B + b) * E.list_cap;
+      for (int q = 0; q < nch; ++q)
+        if (pos + q < E.list_cap) dst[pos + q] = ((uint32_t)i << 8) | (uint32_t)q;
+    }
+  }
+}
+
+__global__ void k_add_rows(int64_t row_elems, int rows, const int32_t* __restrict__ src,
+                           int64_t ss, int32_t* __restrict__ dst, int64_t ds) {
+  const int64_t total = row_elems * rows;
+  for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < total;
+       x += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = x / row_elems, e = x - r * row_elems;
+    dst[r * ds + e] += src[r * ss + e];
+  }
+}
+
+int launch_status() {
+  const cudaError_t err = cudaGetLastError();
+  return (int)err;
+}
+
+int grid_for(int64_t total, int threads) {
+  const int64_t cap = (int64_t)sm_count() * 16;
+  int64_t g = (total + threads - 1) / threads;
+  if (g > cap) g = cap;
+  if (g < 1) g = 1;
+  return (int)g;
+}
+
+bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+int check_range(const fis_engine* e, int32_t b0, int32_t nb) {
+  if (b0 < 0 || nb < 1 || (int64_t)b0 + nb > e->batch) return FIS_E_BOUNDS;
+  return FIS_OK;
+}
+
+}  // namespace
+}  // namespace fis
+
+using namespace fis;
+
+extern "C" {
+
+int fis_abi(void) { return FIS_ABI_VERSION; }
+int fis_sizeof_engine(void) { return (int)sizeof(fis_engine); }
+int fis_sizeof_trial(void) { return (int)sizeof(fis_trial); }
+
+int fis_check(const fis_engine* e) {
+  if (!e) return FIS_E_ARG;
+  if (!e->row_ptr || !e->edges || !e->nchunks || !e->v || !e->g || !e->refrac ||
+      !e->flags || !e->rates || !e->trials || !e->lists || !e->list_len ||
+      !e->bits || !e->clock || !e->done)
+    return FIS_E_ARG;
+  if (e->n < 1 || e->n > (1 << 18) || e->batch < 1 || e->nnz < 0) return FIS_E_ARG;
+  if (e->chunk < 128 || (e->chunk % 128) != 0) return FIS_E_ARG;
+  if (e->list_cap < 1) return FIS_E_ARG;
+  if (e->p.lag < 2 || e->p.buf_len != e->p.lag - 1) return FIS_E_ARG;
+  if (e->n_recs < 0 || (e->n_recs > 0 && !e->recs)) return FIS_E_ARG;
+  if (!aligned16(e->edges)) return FIS_E_ALIGN;
+  return FIS_OK;
+}
+
+int fis_block(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps,
+              int32_t* ring, float* spikes_out, int32_t last_group, void* stream) {
+  int rc = fis_check(e);
+  if (rc) return rc;
+  if ((rc = check_range(e, b0, nb))) return rc;
+  if (!ring) return FIS_E_ARG;
+  const int L = e->p.lag;
+  if (k_steps < 1 || k_steps > FIS_MAX_BLOCK || k_steps > L) return FIS_E_BOUNDS;
+  if (e->vstim && k_steps != 1) return FIS_E_BOUNDS;
+  const int nlists = (k_steps + 1) * nb;
+  if (nlists + 1 > kMaxLists) return FIS_E_BOUNDS;
+  cudaStream_t st = (cudaStream_t)stream;
+
+  ScatterArgs A;
+  A.b0 = b0;
+  A.nb = nb;
+  A.nsrc = k_steps;
+  A.u_off = -(int64_t)L;
+  A.slot_mode = 0;
+  A.zero_next = k_steps;
+  A.filter_last = 1;
+  A.ring = ring;
+  const size_t smem = sizeof(int32_t) * (size_t)(nlists + 1);
+  const int sgrid = sm_count() * 4;
+  k_scatter<<<sgrid, kScatThreads, smem, st>>>(*e, A);
+  if ((rc = launch_status())) return rc;
+
+  const int Wd = (e->n + kWarp - 1) / kWarp;
+  const int64_t threads = (int64_t)nb * Wd * kWarp;
+  const int64_t ugrid = (threads + kUpdThreads - 1) / kUpdThreads;
+  if (ugrid > 0x7FFFFFFF) return FIS_E_BOUNDS;
+  k_update<<<(unsigned)ugrid, kUpdThreads, 0, st>>>(*e, b0, nb, k_steps, ring, spikes_out,
+                                                    last_group ? 1 : 0);
+  return launch_status();
+}
+
+int fis_delay_buffer(const fis_engine* e, int32_t b0, int32_t nb, int32_t* scratch,
+                     float* out, void* stream) {
+  int rc = fis_check(e);
+  if (rc) return rc;
+  if ((rc = check_range(e, b0, nb))) return rc;
+  if (!scratch || !out) return FIS_E_ARG;
+  const int R = e->p.buf_len, L = e->p.lag;
+  if ((R + 1) * nb + 1 > kMaxLists) return FIS_E_BOUNDS;
+  cudaStream_t st = (cudaStream_t)stream;
+  // Pending at clock t: spikes of steps t-L .. t-2; step u lands in slot (u+1) % R.
+  ScatterArgs A;
+  A.b0 = b0;
+  A.nb = nb;
+  A.nsrc = R;
+  A.u_off = -(int64_t)L;
+  A.slot_mode = 1;
+  A.zero_next = 0;
+  A.filter_last = 0;
+  A.ring = scratch;
+  const size_t smem = sizeof(int32_t) * (size_t)((R + 1) * nb + 1);
+  k_scatter<<<sm_count() * 4, kScatThreads, smem, st>>>(*e, A);
+  if ((rc = launch_status())) return rc;
+  const int64_t total = (int64_t)nb * R * e->n;
+  k_ring_to_f32<<<grid_for(total, 256), 256, 0, st>>>(*e, b0, nb, scratch, out);
+  return launch_status();
+}
+
+int fis_spikes_f32(const fis_engine* e, int32_t b0, int32_t nb, int64_t step, float* out,
+                   void* stream) {
+  int rc = fis_check(e);
+  if (rc) return rc;
+  if ((rc = check_range(e, b0, nb))) return rc;
+  if (!out) return FIS_E_ARG;
+  const int64_t total = (int64_t)nb * e->n;
+  k_spikes_f32<<<grid_for(total, 256), 256, 0, (cudaStream_t)stream>>>(*e, b0, nb, step, out);
+  return launch_status();
+}
+
+int fis_load_spikes(const fis_engine* e, int32_t b0, int32_t nb, const float* spikes,
+                    void* stream) {
+  int rc = fis_check(e);
+  if (rc) return rc;
+  if ((rc = check_range(e, b0, nb))) return rc;
+  if (!spikes) return FIS_E_ARG;
+  const int Wd = (e->n + kWarp - 1) / kWarp;
+  const int64_t threads = (int64_t)nb * Wd * kWarp;
+  const int64_t grid = (threads + 255) / 256;
+  k_load_spikes<<<(unsigned)grid, 256, 0, (cudaStream_t)stream>>>(*e, b0, nb, spikes);
+  return launch_status();
+}
+
+int fis_add_rows(const fis_engine* e, int32_t nb, int32_t rows, const int32_t* src,
+                 int64_t src_row_stride, int32_t* dst, int64_t dst_row_stride,
+                 void* stream) {
+  if (!e || !src || !dst || nb < 1 || rows < 0) return FIS_E_ARG;
+  if (rows == 0) return FIS_OK;
+  const int64_t row_elems = (int64_t)nb * e->n;
+  if (src_row_stride < row_elems || dst_row_stride < row_elems) return FIS_E_BOUNDS;
+  k_add_rows<<<grid_for(row_elems * rows, 256), 256, 0, (cudaStream_t)stream>>>(
+      row_elems, rows, src, src_row_stride, dst, dst_row_stride);
+  return launch_status();
+}
+
+}  // extern "C"

@@ -1,0 +1,334 @@
+"""Device-resident engine core: B trial slots over one connectome.
+
+``Core`` owns every device buffer of ``include/fis.h``'s ``fis_engine``
+descriptor (allocated once, through torch's caching allocator) and drives the
+two-phase block of ``libfis_b200.so``.  It is the layer under both the
+reference-compatible :class:`fis.sim.Engine` and the batched/serving layers.
+
+Layout in HBM (B slots, N neurons, L = lag = buf_len + 1 = 20 by default):
+
+* connectome: ``row_ptr`` int64 [N+1], packed ``edges`` uint32 [E rounded up
+  to 4] (60.4 MB at E = 15.09 M), ``nchunks`` uint16 [N];
+* state, trial-major [B][N]: ``v, g, refrac`` float32, ``flags`` uint8,
+  ``rates`` float32 -- read once and written once per block of up to 20 steps;
+* spike history: ``lists`` uint32 [L][B][cap], ``list_len`` int32 [2L][B],
+  ``bits`` uint32 [L][B][ceil(N/32)];
+* scratch ring int32 [K][G][N] for one trial group of G slots, reused by every
+  group: sized to stay resident in the 126 MB L2 between the scatter that fills
+  it and the update that drains it.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+from .connectome import Connectome
+
+MODEL_PARAMS = {
+    "tauSyn": 5.0, "tDelay": 1.8, "v0": -52.0, "vReset": -52.0, "vRest": -52.0,
+    "vThreshold": -45.0, "tauMem": 20.0, "tRefrac": 2.2, "scalePoisson": 250,
+    "wScale": 0.275,
+}
+DT = 0.1
+
+# Bytes of scratch ring per trial group that are meant to stay in L2.
+RING_L2_BYTES = 48 << 20
+
+
+def lif_params(p=None) -> _lib.LifParams:
+    """The step's constants, derived as ``Engine.__init__`` derives them.
+
+    ``sim.py:356-366``: each Python double (``DT / tauSyn`` ...) meets a float32
+    tensor, so it is rounded to float32 once; ``1 - DT/tauSyn`` is formed in
+    double first (``sim.py:929``).  The Poisson kick is the float32 product
+    ``w_scale * (1.0 * scalePoisson)`` (``sim.py:859-861``).
+    """
+    p = dict(MODEL_PARAMS if p is None else p)
+    f = np.float32
+    buf_len = int(p["tDelay"] / DT) + 1
+    w = f(p["wScale"])
+    kick = f(w * f(f(1.0) * f(p["scalePoisson"])))
+    return _lib.LifParams(
+        a_syn=float(f(1.0 - DT / p["tauSyn"])), a_mem=float(f(DT / p["tauMem"])),
+        w_scale=float(w), kick=float(kick), prob_scale=float(f(DT / 1000.0)),
+        v_rest=float(f(p["vRest"])), v_reset=float(f(p["vReset"])),
+        v_th=float(f(p["vThreshold"])),
+        refrac_steps=float(f(float(round(p["tRefrac"] / DT)))),
+        buf_len=buf_len, lag=buf_len + 1, pad_=0)
+
+
+def require_cuda(device):
+    dev = torch.device(device)
+    if dev.type != "cuda":
+        raise _lib.KernelUnavailable(
+            "this engine runs on CUDA only (asked for %r); there is no CPU path" % device)
+    if not torch.cuda.is_available():
+        raise _lib.KernelUnavailable("CUDA is not available in this process")
+    return torch.device("cuda", torch.cuda.current_device() if dev.index is None else dev.index)
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+class Core:
+    """B trial slots, their state on the device, and the block launcher."""
+
+    def __init__(self, conn: Connectome, batch: int, params=None, device="cuda",
+                 group=None, chunk=None, max_block=_lib.FIS_MAX_BLOCK):
+        self.device = require_cuda(device)
+        self.lib = _lib.load()
+        conn.check_bounds()
+        ex = conn.exactness()
+        if not ex["ok"]:
+            raise _lib.KernelUnavailable(
+                "max |row sum| %.0f >= 2**24: integer accumulation would not be "
+                "exact for this matrix" % ex["max_abs_row_sum"])
+        self.conn = conn
+        self.n = n = int(conn.n)
+        self.batch = B = int(batch)
+        if B < 1:
+            raise ValueError("batch must be >= 1")
+        self.pdict = dict(MODEL_PARAMS if params is None else params)
+        self.P = lif_params(self.pdict)
+        self.v0 = float(np.float32(self.pdict["v0"]))
+        L = self.lag = int(self.P.lag)
+        self.buf_len = int(self.P.buf_len)
+        self.max_block = max(1, min(int(max_block), _lib.FIS_MAX_BLOCK, L))
+        dev = self.device
+
+        deg = conn.out_degree()
+        maxdeg = int(deg.max()) if n else 0
+        if chunk is None:
+            chunk = max(256, 128 * math.ceil(maxdeg / (255 * 128)))
+        if chunk % 128 or chunk < 128 or math.ceil(maxdeg / chunk) > 256:
+            raise ValueError("chunk %d does not cover rows of %d edges in 256 pieces"
+                             % (chunk, maxdeg))
+        self.chunk = int(chunk)
+        nch = np.where(deg > 0, -(-deg // self.chunk), 0).astype(np.int64)
+        self.list_cap = max(1, int(nch.sum()))
+
+        packed = conn.packed()
+        nnz = packed.shape[0]
+        nnz4 = max(4, (nnz + 3) // 4 * 4)
+        edges = np.zeros(nnz4, dtype=np.uint32)
+        edges[:nnz] = packed
+        with torch.cuda.device(dev):
+            self.row_ptr = torch.from_numpy(conn.row_ptr.astype(np.int64)).to(dev)
+            self.edges = torch.from_numpy(edges.view(np.int32)).to(dev)
+            self.nchunks = torch.from_numpy(nch.astype(np.int16)).to(dev)
+            self.v = torch.full((B, n), self.v0, dtype=torch.float32, device=dev)
+            self.g = torch.zeros((B, n), dtype=torch.float32, device=dev)
+            self.refrac = torch.full((B, n), self.P.refrac_steps, dtype=torch.float32, device=dev)
+            self.flags = torch.zeros((B, n), dtype=torch.uint8, device=dev)
+            self.rates = torch.zeros((B, n), dtype=torch.float32, device=dev)
+            self.trials_dev = torch.zeros(B * ctypes.sizeof(_lib.Trial), dtype=torch.uint8,
+                                          device=dev)
+            self.lists = torch.zeros((L, B, self.list_cap), dtype=torch.int32, device=dev)
+            self.list_len = torch.zeros((2 * L, B), dtype=torch.int32, device=dev)
+            self.words = (n + 31) // 32
+            self.bits = torch.zeros((L, B, self.words), dtype=torch.int32, device=dev)
+            self.clock = torch.zeros(1, dtype=torch.int64, device=dev)
+            self.done = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.trials = (_lib.Trial * B)()
+        for b in range(B):
+            self.trials[b].start = 0
+            self.trials[b].end = 2 ** 62
+            self.trials[b].v_clamp = float(np.float32(self.pdict["vReset"]))
+            self.trials[b].stream = b
+            self.trials[b].rec = -1
+        self._trials_dirty = True
+        self.recs = []          # recording buffers (int32 [n_bins][N])
+        self._recs_ptrs = None  # device array of their addresses
+        self.step = 0           # host mirror of the device clock
+        self.pending = None     # (first step, int32 [buf_len][B][N]) after restore
+        self.set_group(group)
+
+        self.desc = _lib.EngineDesc()
+        d = self.desc
+        d.row_ptr = self.row_ptr.data_ptr()
+        d.edges = self.edges.data_ptr()
+        d.nchunks = self.nchunks.data_ptr()
+        d.v, d.g, d.refrac = self.v.data_ptr(), self.g.data_ptr(), self.refrac.data_ptr()
+        d.flags = self.flags.data_ptr()
+        d.rates = self.rates.data_ptr()
+        d.vstim = None
+        d.trials = self.trials_dev.data_ptr()
+        d.lists = self.lists.data_ptr()
+        d.list_len = self.list_len.data_ptr()
+        d.bits = self.bits.data_ptr()
+        d.clock = self.clock.data_ptr()
+        d.done = self.done.data_ptr()
+        d.recs = None
+        d.nnz = nnz
+        d.list_cap = self.list_cap
+        d.n, d.batch, d.chunk, d.n_recs = n, B, self.chunk, 0
+        d.p = self.P
+        _lib.check(self.lib.fis_check(ctypes.byref(d)), "fis_check")
+
+    # --- configuration ---------------------------------------------------
+
+    def set_group(self, group=None):
+        """Trial-group size G of the scratch ring [K][G][N] (None: fit in L2)."""
+        if group is None:
+            group = max(1, RING_L2_BYTES // (self.max_block * self.n * 4))
+        self.group = int(max(1, min(int(group), self.batch)))
+        with torch.cuda.device(self.device):
+            self.ring = torch.zeros((self.max_block, self.group, self.n), dtype=torch.int32,
+                                    device=self.device)
+
+    def set_recordings(self, bufs):
+        """Recording buffers, each int32 [n_bins][N]; trials point at them by index."""
+        self.recs = list(bufs)
+        if self.recs:
+            ptrs = torch.tensor([b.data_ptr() for b in self.recs], dtype=torch.int64)
+            self._recs_ptrs = ptrs.to(self.device)
+            self.desc.recs = self._recs_ptrs.data_ptr()
+        else:
+            self._recs_ptrs = None
+            self.desc.recs = None
+        self.desc.n_recs = len(self.recs)
+
+    def _sync_trials(self):
+        if self._trials_dirty:
+            host = torch.frombuffer(bytearray(bytes(self.trials)), dtype=torch.uint8)
+            self.trials_dev.copy_(host)
+            self._trials_dirty = False
+
+    def mark_trials(self):
+        self._trials_dirty = True
+
+    # --- slots -------------------------------------------------------------
+
+    def reset_slots(self, rows):
+        """Initial state for slots ``rows`` (a slice or index tensor).
+
+        ``v = v0``, ``g = 0``, ``refrac = refrac_steps`` of each neuron (0 under
+        FIS_FL_NOREFRAC), as ``Engine.__init__`` (sim.py:383-388); the slot's
+        spike history is emptied so nothing of a previous occupant is delivered.
+        """
+        self.v[rows] = self.v0
+        self.g[rows] = 0.0
+        nore = (self.flags[rows] & _lib.FIS_FL_NOREFRAC) != 0
+        self.refrac[rows] = torch.where(nore, torch.zeros((), device=self.device),
+                                        torch.full((), self.P.refrac_steps, device=self.device))
+        self.list_len[:, rows] = 0
+
+    # --- stepping ------------------------------------------------------------
+
+    def block(self, k, spikes_out=None, stream=None):
+        """Advance every slot by ``k`` steps (1 <= k <= max_block)."""
+        k = int(k)
+        if not 1 <= k <= self.max_block:
+            raise ValueError("block of %d steps; 1..%d allowed" % (k, self.max_block))
+        self._sync_trials()
+        st = (stream or torch.cuda.current_stream(self.device)).cuda_stream
+        sp = ctypes.c_void_p(spikes_out.data_ptr()) if spikes_out is not None else None
+        B, G = self.batch, self.group
+        for g0 in range(0, B, G):
+            nb = min(G, B - g0)
+            if self.pending is not None:
+                self._apply_pending(g0, nb, k, st)
+            rc = self.lib.fis_block(ctypes.byref(self.desc), g0, nb, k,
+                                    ctypes.c_void_p(self.ring.data_ptr()), sp,
+                                    1 if g0 + nb == B else 0, ctypes.c_void_p(st))
+            _lib.check(rc, "fis_block")
+        self.step += k
+        if self.pending is not None and self.step >= self.pending[0] + self.buf_len:
+            self.pending = None
+
+    def _apply_pending(self, g0, nb, k, st):
+        p0, rows = self.pending
+        t0 = self.step
+        lo, hi = max(t0, p0), min(t0 + k, p0 + self.buf_len)
+        if lo >= hi:
+            return
+        n = self.n
+        src = rows[lo - p0, g0]  # [nb][N] starts here; row stride B*N
+        # the kernel's ring for this group is [k][nb][N]: row stride nb*N
+        rc = self.lib.fis_add_rows(ctypes.byref(self.desc), nb, hi - lo,
+                                   ctypes.c_void_p(src.data_ptr()), self.batch * n,
+                                   ctypes.c_void_p(self.ring.data_ptr() + (lo - t0) * nb * n * 4),
+                                   nb * n, ctypes.c_void_p(st))
+        _lib.check(rc, "fis_add_rows")
+
+    def advance(self, steps, spikes_out=None):
+        """``steps`` steps in blocks of at most ``max_block``."""
+        left = int(steps)
+        while left > 0:
+            k = min(left, self.max_block)
+            self.block(k, spikes_out=spikes_out if k == left else None)
+            left -= k
+
+    # --- readouts -------------------------------------------------------------
+
+    def spikes_at(self, step=None, out=None):
+        """Spikes of global step ``step`` (default: the last one) as float [B][N]."""
+        step = self.step - 1 if step is None else int(step)
+        if not (self.step - self.lag <= step < self.step) or step < 0:
+            raise ValueError("step %d is not among the last %d" % (step, self.lag))
+        if out is None:
+            out = torch.empty((self.batch, self.n), dtype=torch.float32, device=self.device)
+        rc = self.lib.fis_spikes_f32(ctypes.byref(self.desc), 0, self.batch, step,
+                                     ctypes.c_void_p(out.data_ptr()),
+                                     ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream))
+        _lib.check(rc, "fis_spikes_f32")
+        return out
+
+    def delay_buffer(self):
+        """The reference's ``delay_buffer`` [B][buf_len][N] float32 (sim.py:385)."""
+        self._sync_trials()
+        R, n, B = self.buf_len, self.n, self.batch
+        out = torch.empty((B, R, n), dtype=torch.float32, device=self.device)
+        per = max(1, min(B, (256 << 20) // (R * n * 4)))
+        st = torch.cuda.current_stream(self.device).cuda_stream
+        for b0 in range(0, B, per):
+            nb = min(per, B - b0)
+            scratch = torch.zeros((R, nb, n), dtype=torch.int32, device=self.device)
+            if self.pending is not None:
+                p0, rows = self.pending
+                for j in range(R):
+                    s = p0 + j
+                    if s >= self.step:
+                        scratch[s % R] += rows[j, b0:b0 + nb]
+            rc = self.lib.fis_delay_buffer(ctypes.byref(self.desc), b0, nb,
+                                           ctypes.c_void_p(scratch.data_ptr()),
+                                           ctypes.c_void_p(out[b0].data_ptr()),
+                                           ctypes.c_void_p(st))
+            _lib.check(rc, "fis_delay_buffer")
+        return out
+
+    # --- restore path -----------------------------------------------------------
+
+    def load_state(self, step, v=None, g=None, refrac=None, spikes=None, ring_counts=None):
+        """Put a state in place at global step ``step`` (restore path).
+
+        ``ring_counts`` int32 [B][buf_len][N] in the reference's slot order:
+        slot ``s % buf_len`` holds the input of step ``s``.  ``spikes`` are the
+        spikes of step ``step - 1`` and are queued for delivery.
+        """
+        step = int(step)
+        self.clock.fill_(step)
+        self.step = step
+        for dst, src in ((self.v, v), (self.g, g), (self.refrac, refrac)):
+            if src is not None:
+                dst.copy_(src)
+        self.list_len.zero_()
+        self.bits.zero_()
+        if ring_counts is not None:
+            R = self.buf_len
+            order = [(step + j) % R for j in range(R)]
+            rows = ring_counts.permute(1, 0, 2)[order].contiguous()
+            self.pending = (step, rows) if bool(rows.any()) else None
+        else:
+            self.pending = None
+        if spikes is not None and step >= 1:
+            rc = self.lib.fis_load_spikes(ctypes.byref(self.desc), 0, self.batch,
+                                          ctypes.c_void_p(spikes.contiguous().data_ptr()),
+                                          ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream))
+            _lib.check(rc, "fis_load_spikes")

@@ -1,0 +1,217 @@
+/*
+ * fis.h -- C ABI of the B200 LIF engine for fly-in-silico's whole-brain step.
+ *
+ * Two families of entry points live here.
+ *
+ * 1. Drop-in replacements for the reference's own event-SpMV FFI
+ *    (lab/flybrain/ev_spmv.cu:114-137, bound by lab/flybrain/evspmv.py:832-930
+ *    through ctypes): same names, same argument meaning, same return
+ *    convention (a cudaError_t code, 0 = success).  A reference build can load
+ *    this library in place of its own DLL.
+ *
+ * 2. The fused engine (fis_*), which replaces the reference's per-step Python
+ *    body Engine._core (lab/flybrain/sim.py:863-953) and the Poisson drive
+ *    Engine._poisson (sim.py:848-861).  Every buffer is owned by the caller
+ *    and passed as a device pointer; nothing here allocates device memory.
+ *    Every call takes a CUDA stream and returns a status instead of trapping.
+ *
+ * Status codes: 0 = success, a positive value is the cudaError_t of a failed
+ * launch, a negative value is one of FIS_E_* (argument checks on the host,
+ * before anything is launched).
+ */
+#ifndef FIS_H
+#define FIS_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FIS_ABI_VERSION 1
+
+/* Largest number of steps one block may advance (registers per thread). */
+#define FIS_MAX_BLOCK 20
+
+enum {
+  FIS_OK = 0,
+  FIS_E_ARG = -1,     /* a pointer is null or a size is out of range */
+  FIS_E_BOUNDS = -2,  /* a trial range, block length or slot is out of range */
+  FIS_E_ALIGN = -3    /* an array is not 16-byte aligned */
+};
+
+/* Per-neuron flag bits, one byte per (trial, neuron). */
+enum {
+  FIS_FL_FIRE_OFF = 1u << 0, /* m_fire = 0: the spike is not emitted        */
+  FIS_FL_OUT_OFF = 1u << 1,  /* m_out  = 0: the spike reaches no synapse    */
+  FIS_FL_IN_OFF = 1u << 2,   /* m_in   = 0: delayed input is discarded      */
+  FIS_FL_HOLD = 1u << 3,     /* m_hold = 0, v_hold = the trial's v_clamp    */
+  FIS_FL_NOREFRAC = 1u << 4, /* refrac_steps = 0 (driven neurons)           */
+  FIS_FL_SILENCED = 1u << 5  /* per-trial silencing: in and out both off    */
+};
+
+/*
+ * Model constants, each computed once on the host exactly as the reference
+ * derives it (sim.py:356-366): the Python double value cast to float32.
+ */
+typedef struct fis_lif_params {
+  float a_syn;        /* f32(1 - dt/tauSyn)                                  */
+  float a_mem;        /* f32(dt/tauMem)                                      */
+  float w_scale;      /* f32(wScale), mV per synapse                         */
+  float kick;         /* f32(wScale) * f32(scalePoisson), a float32 product  */
+  float prob_scale;   /* f32(dt/1000)                                        */
+  float v_rest;
+  float v_reset;
+  float v_th;
+  float refrac_steps; /* f32(round(tRefrac/dt))                              */
+  int32_t buf_len;    /* int(tDelay/dt) + 1, the reference's ring length     */
+  int32_t lag;        /* buf_len + 1: steps from a spike to its g update     */
+  int32_t pad_;
+} fis_lif_params;
+
+/* One trial slot.  Times are global engine steps. */
+typedef struct fis_trial {
+  uint64_t seed;      /* Philox key of this trial's Poisson drive            */
+  int64_t start;      /* global step at which the trial's own step 0 runs    */
+  int64_t end;        /* first global step that is not simulated             */
+  float v_clamp;      /* v_hold value of neurons under FIS_FL_HOLD           */
+  uint32_t stream;    /* Philox counter word 3 (the trial's lane)            */
+  int32_t rec;        /* recording buffer index, -1 = no recording           */
+  int32_t bin_steps;  /* own steps per recording bin                         */
+  int32_t n_bins;     /* bins in the recording buffer                        */
+  int32_t pad_;
+} fis_trial;
+
+/*
+ * The engine descriptor.  All pointers are device pointers owned by the
+ * caller.  Layouts (B = batch, N = n, L = params.lag, W = ceil(N/32)):
+ *   row_ptr  int64 [N+1]       CSR by presynaptic neuron
+ *   edges    uint32 [nnz4]     post << 14 | (count & 0x3fff), 16-byte aligned,
+ *                              nnz4 = nnz rounded up to a multiple of 4
+ *   nchunks  uint16 [N]        ceil(out_degree / chunk), 0 for no edges
+ *   v, g, refrac  float [B][N] the reference's v, conductance, refrac
+ *   flags    uint8 [B][N]      FIS_FL_* bits
+ *   rates    float [B][N]      Poisson rate in Hz, read once per block
+ *   vstim    float [B][N]      or NULL: an external drive (the reference's
+ *                              voltage_stim, sim.py:863) replacing the Philox
+ *                              draw; only 1-step blocks may use it
+ *   trials   fis_trial [B]
+ *   lists    uint32 [L][B][list_cap]  spike entries pre << 8 | chunk
+ *   list_len int32 [2L][B]     entries per (step mod 2L, trial)
+ *   bits     uint32 [L][B][W]  spike raster of the last L steps
+ *   clock    int64 [1]         global steps completed (device-side)
+ *   done     uint32 [1]        block-completion counter, zero between calls
+ *   recs     int32* [n_recs]   recording buffers [n_bins][N]
+ */
+typedef struct fis_engine {
+  const int64_t* row_ptr;
+  const uint32_t* edges;
+  const uint16_t* nchunks;
+  float* v;
+  float* g;
+  float* refrac;
+  uint8_t* flags;
+  const float* rates;
+  const float* vstim;
+  const fis_trial* trials;
+  uint32_t* lists;
+  int32_t* list_len;
+  uint32_t* bits;
+  int64_t* clock;
+  uint32_t* done;
+  int32_t* const* recs;
+  int64_t nnz;
+  int64_t list_cap;
+  int32_t n;
+  int32_t batch;
+  int32_t chunk;      /* edges per scatter work item, a multiple of 128     */
+  int32_t n_recs;
+  fis_lif_params p;
+} fis_engine;
+
+/* ---- family 1: the reference's event-SpMV FFI ------------------------- */
+
+/* out[b, col[k]] += val[k] * sp[b, pre] * mo[b, pre] over the CSR rows of
+ * spiking presynaptic neurons.  Replaces ev_spmv_i32 (ev_spmv.cu:114-122).
+ * `threads` is accepted for signature compatibility; the launch shape is the
+ * library's own.  Returns a cudaError_t code. */
+int ev_spmv_i32(const int* crow, const int* col, const float* val,
+                const float* sp, const float* mo, float* out, int n,
+                int batch, int threads, void* stream);
+
+/* Same with 64-bit indices.  Replaces ev_spmv_i64 (ev_spmv.cu:124-132). */
+int ev_spmv_i64(const long long* crow, const long long* col,
+                const float* val, const float* sp, const float* mo,
+                float* out, int n, int batch, int threads, void* stream);
+
+/* ABI tag checked by the loader.  Replaces ev_spmv_abi (ev_spmv.cu:136-137),
+ * which returns 3; this library returns the same value. */
+int ev_spmv_abi(void);
+
+/* ---- family 2: the fused engine ---------------------------------------- */
+
+/* ABI version of the fis_* family (FIS_ABI_VERSION). */
+int fis_abi(void);
+
+/* Size of fis_engine / fis_trial as compiled, for the binding's check. */
+int fis_sizeof_engine(void);
+int fis_sizeof_trial(void);
+
+/* Host-side validation of a descriptor (no device access).  Returns FIS_OK
+ * or a FIS_E_* code.  Mirrors Events._check_bounds (evspmv.py:1057-1113)
+ * for what can be checked without reading device memory. */
+int fis_check(const fis_engine* e);
+
+/*
+ * Advance the trials in slots [b0, b0+nb) by one block of k_steps steps
+ * (1 <= k_steps <= min(FIS_MAX_BLOCK, lag)).  Two launches: the scatter of
+ * the spikes that reach these steps through the delay (CSR rows of spiking
+ * neurons, int32 atomics into `ring`), then the fused neuron update of all
+ * k_steps steps (refractory gate, delayed input, conductance, Poisson drive,
+ * membrane, hold, threshold, reset).  Replaces one call of Engine.step per
+ * step (sim.py:745-771, 863-953).
+ *   ring        int32 [k_steps][nb][N], all zero on entry, all zero on exit
+ *   spikes_out  float [B][N] or NULL: the spikes of the block's last step
+ *   last_group  nonzero when this call completes the block for all trial
+ *               groups; the device clock then advances by k_steps
+ */
+int fis_block(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps,
+              int32_t* ring, float* spikes_out, int32_t last_group,
+              void* stream);
+
+/*
+ * Write the reference's pending delay ring (Engine.delay_buffer,
+ * sim.py:385) for slots [b0, b0+nb): out float [nb][buf_len][N], slot
+ * s mod buf_len holding w_scale * the counts that reach step s (from the
+ * spikes of step s - lag), for the pending steps s = clock .. clock+buf_len-1.
+ * `scratch` int32 [buf_len][nb][N] is accumulated into: the caller zeroes it
+ * and may preload counts that are pending from a restored ring.
+ */
+int fis_delay_buffer(const fis_engine* e, int32_t b0, int32_t nb,
+                     int32_t* scratch, float* out, void* stream);
+
+/* Expand the spike bits of global step `step` into float 0/1 [nb][N]. */
+int fis_spikes_f32(const fis_engine* e, int32_t b0, int32_t nb, int64_t step,
+                   float* out, void* stream);
+
+/*
+ * Load a pending spike list from a float 0/1 spike tensor [nb][N] as the
+ * spikes of global step clock-1 (restore path; the reference keeps these in
+ * Engine.spikes).  Entries are written unfiltered, as the block that
+ * consumes them filters by m_out.  Also writes the raster bits.
+ */
+int fis_load_spikes(const fis_engine* e, int32_t b0, int32_t nb,
+                    const float* spikes, void* stream);
+
+/* dst[r][b][i] += src[r][b][i] for r < rows, b < nb, i < N, with the row
+ * strides given in elements (restore path: pending delayed input that a
+ * restored delay ring holds for the next buf_len steps). */
+int fis_add_rows(const fis_engine* e, int32_t nb, int32_t rows,
+                 const int32_t* src, int64_t src_row_stride, int32_t* dst,
+                 int64_t dst_row_stride, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FIS_H */

@@ -1,0 +1,119 @@
+"""Generate the golden parity fixtures by running the REFERENCE engine.
+
+Runs only where the reference tree is present (it is read, never copied):
+
+    python tests/golden/make_golden.py [scenario ...]
+
+For every scenario of ``tests/scenarios.py`` it builds the reference's own
+``sim.Engine`` (``lab/flybrain/sim.py:348``) on CPU with the synthetic
+connectome as its weight matrix, silences through the reference's own
+``sim._silence`` (``sim.py:324-336``), applies the mask plan through
+``Engine.set_masks`` (``sim.py:510``), and steps it with ``Engine._core``
+(``sim.py:863``) fed by the shared Philox input tape, the way the
+reference's parity probes drive it.  It records the spike raster of every step
+and fingerprints of the full state at milestones, plus the final state arrays
+for the small scenarios.  The fixtures pin the C oracle (CPU tests) and the
+CUDA engine (GPU tests).
+"""
+
+from __future__ import annotations
+
+import hashlib
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+REF_LAB = Path("/root/reference/lab")
+sys.path.insert(0, str(ROOT / "fly-in-silico_b200"))
+sys.path.insert(0, str(ROOT / "tests"))
+sys.path.insert(0, str(ROOT))
+
+import scenarios as S  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+
+
+def fp(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()[:16]
+
+
+def run_reference(name):
+    import torch
+
+    sys.path.insert(0, str(REF_LAB))
+    from flybrain import sim
+
+    torch.set_num_threads(8)
+    sc = S.SCENARIOS[name]
+    conn = S.connectome(sc)
+    n, B = sc["n"], sc["batch"]
+    W = conn.to_torch_weights()
+    sil = S.silenced(sc)
+    if sil.size:
+        W = sim._silence(W, sil, n)
+    drv = S.driven(sc)
+    eng = sim.Engine(W, n, params=sc["params"], device="cpu", batch=B,
+                     seed=sc["seed"], no_refractory=drv, spmv=sim.SPMV_CSR)
+    rates = S.rates_matrix(sc)
+    seeds = np.full(B, sc["seed"], dtype=np.uint64)
+    streams = np.arange(B, dtype=np.uint32)
+    plan = dict(sc["plan"])
+    idx = S.busy(sc)
+    nbytes = (n + 7) // 8
+    raster = np.zeros((sc["steps"], B, nbytes), dtype=np.uint8)
+    marks = {}
+    t0 = time.time()
+    for step in range(sc["steps"]):
+        what = plan.get(step)
+        if what is not None:
+            eng.set_masks(**S.mask_call(what, idx))
+        tape = O.drive_tape(rates, seeds, streams, np.full(B, step, np.int64),
+                            sc["params"])
+        sp = eng._core(torch.from_numpy(tape)).numpy()
+        raster[step] = np.packbits(sp != 0, axis=1, bitorder="little")
+        if step + 1 in S.MILESTONES or step + 1 == sc["steps"]:
+            marks[step + 1] = {
+                "v": fp(eng.v.numpy()), "g": fp(eng.conductance.numpy()),
+                "refrac": fp(eng.refrac.numpy()), "spikes": fp(eng.spikes.numpy()),
+                "ring": fp(eng.delay_buffer.numpy()), "ptr": int(eng.ptr),
+            }
+    wall = time.time() - t0
+    out = {
+        "raster_bits": raster,
+        "marks_steps": np.array(sorted(marks), dtype=np.int64),
+        "marks": np.array([[marks[k][f] for f in ("v", "g", "refrac", "spikes", "ring")]
+                           for k in sorted(marks)]),
+        "marks_ptr": np.array([marks[k]["ptr"] for k in sorted(marks)], dtype=np.int64),
+        "total_spikes": np.int64(int(np.unpackbits(raster, bitorder="little").sum())),
+        "ref_ms_per_step": np.float64(wall * 1000.0 / sc["steps"]),
+    }
+    if n <= 5000:
+        out.update(v=eng.v.numpy(), g=eng.conductance.numpy(), refrac=eng.refrac.numpy(),
+                   spikes=eng.spikes.numpy(), ring=eng.delay_buffer.numpy(),
+                   ptr=np.int64(eng.ptr))
+    else:
+        # full size: the raster as (step, trial, neuron) triples (it is sparse)
+        st, b, i = np.nonzero(np.unpackbits(raster, axis=2, bitorder="little")[:, :, :n])
+        out.pop("raster_bits")
+        out.update(spike_step=st.astype(np.int32), spike_trial=b.astype(np.int16),
+                   spike_neuron=i.astype(np.int32))
+    path = OUT / ("%s.npz" % name)
+    np.savez_compressed(path, **out)
+    print("%-14s %5d steps, %6d spikes, reference %.1f ms/step -> %s (%d KB)"
+          % (name, sc["steps"], int(out["total_spikes"]), wall * 1000 / sc["steps"],
+             path.name, path.stat().st_size // 1024))
+
+
+def main(argv):
+    names = argv or list(S.SCENARIOS)
+    O.build()
+    for name in names:
+        run_reference(name)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:])

@@ -1,0 +1,94 @@
+"""Parity scenarios shared by the golden generator and the tests.
+
+Each scenario is a seeded synthetic connectome, a Poisson drive on a seeded
+subset, a model-parameter set and a schedule of ``set_masks`` calls applied
+before given steps.  Everything is derived from the integers below, so the
+reference (here), the oracle and the CUDA engine all see the same inputs.
+The mask windows follow the reference's own parity probe
+(``lab/probe/lif_event.py:233-243``): each intervention alone and all four
+together, with windows longer than the 19/20-step delay tails.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+ALT_PARAMS = {
+    "tauSyn": 4.0, "tDelay": 1.0, "v0": -55.0, "vReset": -58.0, "vRest": -52.5,
+    "vThreshold": -46.3, "tauMem": 17.0, "tRefrac": 1.3, "scalePoisson": 200,
+    "wScale": 0.31,
+}
+
+LIF_EVENT_PLAN = [(60, "fire"), (100, "clear"), (130, "out"), (170, "clear"),
+                  (200, "inc"), (230, "clear"), (250, "hold"), (280, "clear"),
+                  (300, "all"), (340, "clear")]
+
+SCENARIOS = {
+    "small_b1": dict(n=2048, e=2048 * 100, conn_seed=1, batch=1, steps=400,
+                     seed=5, drive_k=300, drive_seed=2, rates=[150.0],
+                     plan=[], params=None),
+    "batch3_masks": dict(n=3000, e=3000 * 109, conn_seed=3, batch=3, steps=360,
+                         seed=9, drive_k=400, drive_seed=4,
+                         rates=[60.0, 150.0, 240.0], plan=LIF_EVENT_PLAN,
+                         params=None),
+    "silenced_b2": dict(n=2500, e=2500 * 110, conn_seed=5, batch=2, steps=300,
+                        seed=13, drive_k=350, drive_seed=6, rates=[200.0, 120.0],
+                        silenced_k=60, silenced_seed=8, plan=[], params=None),
+    "alt_params": dict(n=2200, e=2200 * 105, conn_seed=7, batch=2, steps=320,
+                       seed=21, drive_k=320, drive_seed=10, rates=[180.0, 90.0],
+                       plan=[(40, "hold_clamp"), (90, "clear"), (150, "all"),
+                             (200, "clear")], params=ALT_PARAMS),
+    # The plain single-trial configuration at full size (1,000 steps).
+    "full_cfg0": dict(n=138_639, e=15_091_983, conn_seed=0, batch=1, steps=1000,
+                      seed=0, drive_k=2249, drive_seed=1, rates=[150.0], plan=[],
+                      params=None),
+}
+
+MILESTONES = (1, 10, 19, 20, 21, 40, 100, 200, 300, 400, 500, 1000)
+
+
+def connectome(sc):
+    import fis.connectome as C
+
+    return C.synthetic(n=sc["n"], e=sc["e"], seed=sc["conn_seed"])
+
+
+def driven(sc):
+    rng = np.random.default_rng(sc["drive_seed"])
+    return np.sort(rng.choice(sc["n"], size=sc["drive_k"], replace=False)).astype(np.int64)
+
+
+def silenced(sc):
+    if not sc.get("silenced_k"):
+        return np.zeros(0, dtype=np.int64)
+    rng = np.random.default_rng(sc["silenced_seed"])
+    return np.sort(rng.choice(sc["n"], size=sc["silenced_k"], replace=False)).astype(np.int64)
+
+
+def busy(sc):
+    """Neurons the mask plan acts on: 300 driven ones and 300 others."""
+    d = driven(sc)
+    rng = np.random.default_rng(sc["drive_seed"] + 1000)
+    others = np.setdiff1d(np.arange(sc["n"]), d)
+    extra = rng.choice(others, size=min(300, others.size), replace=False)
+    return np.concatenate([d[:300], np.sort(extra)]).astype(np.int64)
+
+
+def rates_matrix(sc):
+    r = np.zeros((sc["batch"], sc["n"]), dtype=np.float32)
+    d = driven(sc)
+    for b, hz in enumerate(sc["rates"]):
+        r[b, d] = hz
+    return r
+
+
+def mask_call(what, idx):
+    """Keyword arguments of the ``set_masks`` call for one plan entry."""
+    if what == "clear":
+        return dict(fire=[], out=[], inc=[], hold=[])
+    if what == "all":
+        return dict(fire=idx[:150], out=idx[150:300], inc=idx[300:450],
+                    hold=idx[450:600])
+    if what == "hold_clamp":
+        return dict(hold=idx[:200], v_clamp=-61.5)
+    return {what: idx}

@@ -1,0 +1,139 @@
+"""Host-side logic that needs no GPU: connectome, packing, params, ABI exports."""
+
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import fis._lib as L
+import fis.connectome as C
+from fis.engine import lif_params
+from oracle import oracle as O
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def test_synthetic_full_size_statistics():
+    c = C.synthetic()
+    d = c.out_degree()
+    assert c.n == C.N_FLYWIRE and c.nnz == C.E_FLYWIRE
+    assert abs(d.mean() - C.E_FLYWIRE / C.N_FLYWIRE) < 1e-9
+    assert d.max() <= c.n - 1 and d.min() >= 1
+    pre = np.repeat(np.arange(c.n), d)
+    assert not np.any(pre == c.col)                      # no self-loops
+    assert np.all(np.diff(pre.astype(np.int64) * c.n + c.col) > 0)  # unique, sorted
+    assert c.cnt.min() >= -2400 and c.cnt.max() <= 2400 and not np.any(c.cnt == 0)
+    sign = np.sign(c.cnt)
+    assert np.all(sign[c.row_ptr[:-1][d > 0]] == sign[c.row_ptr[1:][d > 0] - 1])  # sign per pre
+    frac_inh = np.mean(sign[c.row_ptr[:-1][d > 0]] < 0)
+    assert 0.28 < frac_inh < 0.32
+    assert c.exactness()["ok"]
+
+
+def test_synthetic_is_deterministic():
+    a = C.synthetic(n=3000, e=300000, seed=4, cache=False)
+    b = C.synthetic(n=3000, e=300000, seed=4, cache=False)
+    assert np.array_equal(a.col, b.col) and np.array_equal(a.cnt, b.cnt)
+    c = C.synthetic(n=3000, e=300000, seed=5, cache=False)
+    assert not np.array_equal(a.col, c.col)
+
+
+def test_packed_roundtrip_and_limits():
+    c = C.synthetic(n=2000, e=150000, seed=2, cache=False)
+    w = c.packed()
+    post = (w >> 14).astype(np.int64)
+    cnt = ((w.astype(np.int64) & 0x3FFF) ^ 0x2000) - 0x2000
+    assert np.array_equal(post, c.col) and np.array_equal(cnt, c.cnt)
+    big = C.Connectome(4, np.array([0, 1, 1, 1, 1]), np.array([1], np.int32),
+                       np.array([9000], np.int32))
+    with pytest.raises(C.ConnectomeError):
+        big.packed()
+
+
+def test_from_weights_roundtrip():
+    import torch
+
+    c = C.synthetic(n=1500, e=90000, seed=9, cache=False)
+    w = c.to_torch_weights()
+    back = C.from_weights(w)
+    assert np.array_equal(back.row_ptr, c.row_ptr)
+    assert np.array_equal(back.col, c.col) and np.array_equal(back.cnt, c.cnt)
+    bad = torch.sparse_coo_tensor(torch.tensor([[0], [1]]), torch.tensor([1.5]), (3, 3))
+    with pytest.raises(C.ConnectomeError):
+        C.from_weights(bad)
+
+
+def test_without_matches_reference_silencing_semantics():
+    c = C.synthetic(n=1200, e=60000, seed=3, cache=False)
+    sil = np.array([5, 17, 400])
+    s = c.without(sil)
+    pre = np.repeat(np.arange(s.n), s.out_degree())
+    assert not np.isin(pre, sil).any() and not np.isin(s.col, sil).any()
+    kept = ~(np.isin(np.repeat(np.arange(c.n), c.out_degree()), sil) | np.isin(c.col, sil))
+    assert s.nnz == int(kept.sum())
+
+
+def test_bounds_check_refuses_bad_csr():
+    c = C.Connectome(3, np.array([0, 1, 2, 2]), np.array([1, 3], np.int32),
+                     np.array([1, 1], np.int32))
+    with pytest.raises(C.ConnectomeError):
+        c.check_bounds()
+
+
+@pytest.mark.parametrize("p", [None, {"tauSyn": 4.0, "tDelay": 1.0, "v0": -55.0, "vReset": -58.0,
+                                      "vRest": -52.5, "vThreshold": -46.3, "tauMem": 17.0,
+                                      "tRefrac": 1.3, "scalePoisson": 200, "wScale": 0.31}])
+def test_params_match_oracle(p):
+    a, b = lif_params(p), O.params(p)
+    for name, _ in b._fields_:
+        assert getattr(a, name) == getattr(b, name), name
+
+
+def test_library_exports_every_declared_symbol():
+    """The C-ABI library loads on a CPU-only host and exports fis.h's symbols."""
+    import fis.build
+
+    fis.build.build()
+    header = (ROOT / "include" / "fis.h").read_text()
+    declared = set(re.findall(r"^int\s+(\w+)\(", header, flags=re.M))
+    assert declared == set(L.EXPORTS)
+    lib = ctypes.CDLL(str(L.LIB_PATH))
+    for name in declared:
+        assert hasattr(lib, name), name
+    L.load()  # ABI and struct-layout checks (no device call)
+    assert lib.ev_spmv_abi() == 3
+
+
+def test_check_rejects_bad_descriptor():
+    lib = L.load()
+    d = L.EngineDesc()
+    assert lib.fis_check(ctypes.byref(d)) == -1  # null pointers
+    assert lib.fis_block(ctypes.byref(d), 0, 1, 1, None, None, 1, None) == -1
+
+
+def test_rate_guard():
+    from fis import sim
+
+    sim.check_rates_hz([0.0, 150.0, 10000.0], "test")
+    for bad in ([10001.0], [-1.0], [float("nan")]):
+        with pytest.raises(sim.RateTooHigh):
+            sim.check_rates_hz(bad, "test")
+
+
+def test_stim_schedule_matches_reference_order():
+    from fis import sim
+
+    s1 = sim.Stimulus(np.array([1, 2]), 100.0, t_on_ms=5.0, t_off_ms=20.0)
+    s2 = sim.Stimulus(np.array([3]), 50.0)
+    ev = sim.stim_schedule([s1, s2], steps=1000)
+    assert [(e[0], e[2]) for e in ev] == [(0, 50.0), (50, 100.0), (200, 0.0)]
+
+
+def test_engine_refuses_cpu_loudly():
+    from fis import evspmv, sim
+
+    c = C.synthetic(n=500, e=20000, seed=1, cache=False)
+    with pytest.raises(evspmv.EventKernelUnavailable):
+        sim.Engine(c, c.n, device="cpu")

@@ -1,0 +1,200 @@
+"""The CUDA engine against the reference's outputs and the oracle, bit for bit.
+
+Every test here runs the engine through its C ABI (``libfis_b200.so`` via
+``fis``) on the inputs the golden fixtures were made from, and compares
+spike rasters and full state with the reference's own results.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+import scenarios as S
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+SMALL = ["small_b1", "batch3_masks", "silenced_b2", "alt_params"]
+
+
+def raster_rows(core, first, last):
+    """Bit rows [step][B][nbytes] of global steps first..last-1 from the engine."""
+    nbytes = (core.n + 7) // 8
+    out = []
+    bits = core.bits.cpu().numpy()
+    for s in range(first, last):
+        row = bits[s % core.lag].view(np.uint8)[:, :nbytes]
+        out.append(row.copy())
+    return out
+
+
+def make_engine(name, graphs=False, group=None):
+    from fis import sim
+
+    sc = S.SCENARIOS[name]
+    conn = S.connectome(sc)
+    eng = sim.build_engine(weights=conn, silenced=S.silenced(sc), params=sc["params"],
+                           batch=sc["batch"], seed=sc["seed"], no_refractory=S.driven(sc),
+                           graphs=graphs, group=group)
+    return sc, eng
+
+
+def final_state_equal(eng, z):
+    checks = {
+        "v": eng.v.cpu().numpy(), "g": eng.conductance.cpu().numpy(),
+        "refrac": eng.refrac.cpu().numpy(), "spikes": eng.spikes.cpu().numpy(),
+        "ring": eng.delay_buffer.cpu().numpy(),
+    }
+    bad = [k for k, a in checks.items() if not np.array_equal(a, z[k])]
+    if int(eng.ptr) != int(z["ptr"]):
+        bad.append("ptr")
+    return bad
+
+
+@pytest.mark.parametrize("name", SMALL)
+@pytest.mark.parametrize("graphs", [False, True])
+def test_step_api_matches_reference(name, graphs, golden):
+    """``Engine.step`` per step, masks between steps, as the reference's probes."""
+    z = golden(name)
+    sc, eng = make_engine(name, graphs=graphs)
+    rates = torch.from_numpy(S.rates_matrix(sc)).cuda()
+    plan = dict(sc["plan"])
+    idx = S.busy(sc)
+    rows = []
+    for step in range(sc["steps"]):
+        if step in plan:
+            eng.set_masks(**S.mask_call(plan[step], idx))
+        sp = eng.step(rates)
+        rows.append(np.packbits(sp.cpu().numpy() != 0, axis=1, bitorder="little"))
+    assert np.array_equal(np.stack(rows), z["raster_bits"])
+    assert final_state_equal(eng, z) == []
+    assert eng.calls == sc["steps"]
+
+
+@pytest.mark.parametrize("name", SMALL)
+def test_tape_driven_core_matches_reference(name, golden):
+    """``Engine._core(voltage_stim)`` with the shared tape (the probes' form)."""
+    z = golden(name)
+    sc, eng = make_engine(name)
+    rates = S.rates_matrix(sc)
+    seeds = np.full(sc["batch"], sc["seed"], dtype=np.uint64)
+    streams = np.arange(sc["batch"], dtype=np.uint32)
+    plan = dict(sc["plan"])
+    idx = S.busy(sc)
+    rows = []
+    for step in range(sc["steps"]):
+        if step in plan:
+            eng.set_masks(**S.mask_call(plan[step], idx))
+        tape = O.drive_tape(rates, seeds, streams, np.full(sc["batch"], step), sc["params"])
+        sp = eng._core(torch.from_numpy(tape).cuda())
+        rows.append(np.packbits(sp.cpu().numpy() != 0, axis=1, bitorder="little"))
+    assert np.array_equal(np.stack(rows), z["raster_bits"])
+    assert final_state_equal(eng, z) == []
+
+
+@pytest.mark.parametrize("name", SMALL)
+@pytest.mark.parametrize("group", [None, 1, 2])
+def test_blocked_stepping_matches_reference(name, group, golden):
+    """Blocks of up to 20 fused steps, split only where the masks change."""
+    z = golden(name)
+    sc, eng = make_engine(name, group=group)
+    core = eng.core
+    core.rates.copy_(torch.from_numpy(S.rates_matrix(sc)))
+    plan = dict(sc["plan"])
+    idx = S.busy(sc)
+    cuts = sorted(set([s for s in plan] + [sc["steps"]]))
+    rows = []
+    step = 0
+    for cut in cuts:
+        if step in plan:
+            eng.set_masks(**S.mask_call(plan[step], idx))
+        while step < cut:
+            k = min(core.max_block, cut - step)
+            core.block(k, spikes_out=eng.spikes)
+            rows += raster_rows(core, step, step + k)
+            step += k
+    eng._spikes_version = eng.spikes._version
+    assert np.array_equal(np.stack(rows), z["raster_bits"])
+    assert final_state_equal(eng, z) == []
+
+
+def test_full_size_config0_matches_reference(golden):
+    """138,639 neurons, 15.09 M edges, 1,000 steps in 20-step blocks."""
+    z = golden("full_cfg0")
+    sc, eng = make_engine("full_cfg0")
+    core = eng.core
+    core.rates.copy_(torch.from_numpy(S.rates_matrix(sc)))
+    rows = []
+    for step in range(0, sc["steps"], 20):
+        core.block(20, spikes_out=eng.spikes)
+        rows += raster_rows(core, step, step + 20)
+    bits = np.unpackbits(np.stack(rows), axis=2, bitorder="little")[:, :, :sc["n"]]
+    st, b, i = np.nonzero(bits)
+    assert np.array_equal(st, z["spike_step"]) and np.array_equal(i, z["spike_neuron"])
+    fps = [O.fingerprint(a) for a in (eng.v.cpu().numpy(), eng.conductance.cpu().numpy(),
+                                      eng.refrac.cpu().numpy(), eng.spikes.cpu().numpy(),
+                                      eng.delay_buffer.cpu().numpy())]
+    assert fps == list(z["marks"][-1])
+
+
+def test_snapshot_restore_continues_bit_exactly():
+    """Continue-from-snapshot equals the uninterrupted run (probe/resume_state.py)."""
+    name = "batch3_masks"
+    sc, a = make_engine(name)
+    rates = torch.from_numpy(S.rates_matrix(sc)).cuda()
+    idx = S.busy(sc)
+    a.set_masks(out=idx[:200], hold=idx[200:300], v_clamp=-60.0)
+    for _ in range(137):
+        a.step(rates)
+    snap = a.snapshot()
+    for _ in range(90):
+        a.step(rates)
+    _, b = make_engine(name)
+    b.restore(snap)
+    for _ in range(90):
+        b.step(rates)
+    for name_ in ("v", "conductance", "refrac", "spikes"):
+        assert torch.equal(getattr(a, name_), getattr(b, name_)), name_
+    assert torch.equal(a.delay_buffer, b.delay_buffer)
+    assert a.ptr == b.ptr
+
+
+def test_restore_drop_one_changes_the_future():
+    """Completeness of the state: dropping any element changes what follows."""
+    name = "small_b1"
+    sc, a = make_engine(name)
+    rates = torch.from_numpy(S.rates_matrix(sc)).cuda()
+    for _ in range(120):
+        a.step(rates)
+    snap = a.snapshot()
+    for _ in range(60):
+        a.step(rates)
+    ref = a.v.clone()
+    for drop in ("v", "conductance", "refrac", "delay_buffer", "spikes", "ptr"):
+        _, b = make_engine(name)
+        for _ in range(7):
+            b.step(rates)
+        b.restore(snap, drop=(drop,))
+        for _ in range(60):
+            b.step(rates)
+        assert not torch.equal(b.v, ref), drop
+
+
+def test_ev_spmv_dropin_exact():
+    """The reference-FFI drop-in equals an exact integer sum."""
+    from fis import evspmv
+
+    c = S.connectome(S.SCENARIOS["batch3_masks"])
+    w = c.to_torch_weights("cuda").to_sparse_csr()
+    B = 3
+    ev = evspmv.Events(w, B, "cuda")
+    g = torch.Generator(device="cpu").manual_seed(3)
+    sp = (torch.rand(B, c.n, generator=g) < 0.05).float().cuda()
+    mo = (torch.rand(B, c.n, generator=g) < 0.9).float().cuda()
+    out = ev.mm(sp, mo).cpu().numpy()
+    x = (sp * mo).cpu().numpy().astype(np.int64)
+    pre = np.repeat(np.arange(c.n), c.out_degree())
+    want = np.zeros((B, c.n), dtype=np.int64)
+    for b in range(B):
+        np.add.at(want[b], c.col, c.cnt.astype(np.int64) * x[b, pre])
+    assert np.array_equal(out, want.astype(np.float32))
