@@ -1,0 +1,369 @@
+"""Benchmark: batched whole-brain LIF trials on B200.
+
+One bench step is one complete batch: 64 trials x 10,000 steps (1 s of
+simulated time each) on the 138,639-neuron, 15,091,983-edge synthetic
+connectome, every trial with its own Philox seed, 500-5,000 stimulated
+neurons at 50-300 Hz and 1-100 silenced neurons.  The metric is simulated
+neuron-steps per second over all GPUs.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Arms:
+  default           the B200 engine (libfis_b200.so); ``value`` is timed with
+                    the inputs resident on the device, ``e2e`` through
+                    ``fis.batch.Batch.run`` with host inputs and host results.
+  --impl reference  the reference's algorithm on the host cores (the C port of
+                    its default csrmv path under oracle/), all threads, on a
+                    bounded sample of the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "fly-in-silico_b200"))
+sys.path.insert(0, str(ROOT))
+
+N_TRIALS = 64
+SIM_STEPS = 10_000
+WORKLOAD = ("batched 64 trials x 10,000 steps (1 s), N=138,639, E=15,091,983 synthetic "
+            "connectome; per trial: own Philox seed, 500-5,000 stimulated at 50-300 Hz, "
+            "1-100 silenced")
+SPEC_SEED = 2024
+CONN_SEED = 0
+# Update-kernel DRAM traffic per launch from the committed ncu capture
+# (profiles/k_update_ncu.md); None until measured.
+NCU_TRAFFIC_PER_LAUNCH = None
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="fis", choices=["fis", "reference"])
+    ap.add_argument("--trials", type=int, default=N_TRIALS)
+    ap.add_argument("--sim-steps", type=int, default=SIM_STEPS)
+    ap.add_argument("--group", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = Path("/tmp/fis_clocks_%d.csv" % os.getpid())
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, smax, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.path.read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        self.path.unlink(missing_ok=True)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def cpu_sample(conn, specs, steps, threads):
+    """The reference's CPU algorithm (csrmv over every edge, the default path)."""
+    import numpy as np
+
+    from oracle import oracle as O
+    from fis.batch import host_rows
+
+    flags, rates = host_rows(specs, conn.n)
+    o = O.Oracle.from_connectome(conn, batch=len(specs), no_refractory=None)
+    o.rates[:] = rates
+    o.refrac_steps[(flags & 16) != 0] = 0.0
+    o.refrac[:] = o.refrac_steps
+    sil = (flags & 32) != 0
+    o.m_out[sil] = 0.0
+    o.m_in[sil] = 0.0
+    o.seeds[:] = np.array([s.seed for s in specs], dtype=np.uint64)
+    o.streams[:] = 0
+    t = time.perf_counter()
+    o.run(steps, mode=O.Oracle.CSRMV, threads=threads)
+    return time.perf_counter() - t
+
+
+def reference_arm(args, rank):
+    if rank != 0:
+        return 0
+    import fis.connectome as C
+    from fis.batch import random_specs
+
+    threads = os.cpu_count() or 1
+    conn = C.synthetic(seed=CONN_SEED)
+    specs = random_specs(conn.n, args.trials, SPEC_SEED, args.sim_steps)
+    sample_steps = 2
+    for _ in range(args.warmup):
+        cpu_sample(conn, specs, sample_steps, threads)
+    times = [cpu_sample(conn, specs, sample_steps, threads) for _ in range(args.steps)]
+    total = sum(times)
+    units = args.trials * conn.n * sample_steps * args.steps
+    value = units / total
+    line = {
+        "impl": "reference", "metric": "batched neuron-steps/s", "value": value,
+        "unit": "neuron-steps/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "trials": args.trials, "sim_steps": args.sim_steps,
+                   "sample": "%d trials x %d steps per bench step" % (args.trials, sample_steps)},
+        "cpu_baseline": {"value": value, "unit": "neuron-steps/s", "cores": threads,
+                         "kind": "port",
+                         "sample": "%d trials x %d steps, csrmv over all edges (the "
+                                   "reference's default CPU path), C port in oracle/"
+                                   % (args.trials, sample_steps)},
+        "e2e": {"value": value, "unit": "neuron-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        return reference_arm(args, rank)
+
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+
+    import fis.connectome as C
+    from fis.batch import Batch, random_specs
+
+    conn = C.synthetic(seed=CONN_SEED)
+    specs = random_specs(conn.n, args.trials, SPEC_SEED + 1000 * rank, args.sim_steps)
+    batch = Batch(conn, args.trials, group=args.group)
+    core = batch.core
+    slots = list(range(args.trials))
+    batch.load(slots, specs)
+
+    def resident_run(events=None, every=1):
+        for b in slots:
+            t = core.trials[b]
+            t.start = core.step
+            t.end = core.step + specs[b].steps
+        core.mark_trials()
+        core.reset_slots(slice(None))
+        for r in batch._recs:
+            r.zero_()
+        core.advance(args.sim_steps, events=events, every=every)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if pg is not None:
+            pg.barrier()
+
+    def max_over_ranks(x):
+        if pg is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        resident_run()
+    blocks = -(-args.sim_steps // core.max_block)
+    upd_per_run = blocks * (-(-args.trials // core.group))
+    n_pairs = 64
+    every = max(1, upd_per_run // n_pairs)
+    events = [[torch.cuda.Event(enable_timing=True) for _ in range(2 * n_pairs)]
+              for _ in range(args.steps)]
+
+    gpu_index = local
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        try:
+            gpu_index = int(vis.split(",")[local])
+        except ValueError:
+            pass
+    sampler = ClockSampler(gpu_index)
+    barrier()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with sampler:
+        time.sleep(0.3)
+        barrier()
+        start.record()
+        for k in range(args.steps):
+            resident_run(events=events[k], every=every)
+        end.record()
+        barrier()
+    ms = max_over_ranks(start.elapsed_time(end))
+    clocks = sampler.summary()
+    durs = []
+    for evs in events:
+        for j in range(n_pairs):
+            d = evs[2 * j].elapsed_time(evs[2 * j + 1])
+            if d > 0:
+                durs.append(d)
+    upd_ms = statistics.mean(durs) if durs else None
+
+    units_rank = args.trials * conn.n * args.sim_steps
+    value = world * units_rank * args.steps / (ms / 1000.0)
+
+    # end to end through the public API: host specs in, host counts out
+    h2d = args.trials * conn.n * (1 + 4) + args.trials * 48 + args.trials * 8
+    d2h = args.trials * conn.n * 4
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        batch.run(specs)
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e = world * units_rank * args.steps / e2e_s
+
+    # the plain single-trial step through the reference-compatible API
+    plain = None
+    if rank == 0:
+        from fis import sim
+
+        rng = np.random.default_rng(1)
+        drive = np.sort(rng.choice(conn.n, 2249, replace=False))
+        eng = sim.build_engine(weights=conn, batch=1, seed=0, no_refractory=drive, graphs=True)
+        rates = torch.zeros(1, conn.n, device="cuda")
+        rates[0, torch.as_tensor(drive, device="cuda")] = 150.0
+        for _ in range(50):
+            eng.step(rates)
+        torch.cuda.synchronize()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n_plain = 2000
+        s0.record()
+        for _ in range(n_plain):
+            eng.step(rates)
+        s1.record()
+        torch.cuda.synchronize()
+        pms = s0.elapsed_time(s1) / n_plain
+        plain = {"value": conn.n / (pms / 1000.0), "unit": "neuron-steps/s",
+                 "ms_per_step": pms,
+                 "how": "Engine.step() per 0.1 ms tick, 1 trial, CUDA graph, 2,249 driven "
+                        "at 150 Hz"}
+        del eng
+
+    hbm, peak_kind = peaks()
+    alg = None
+    roof = None
+    if upd_ms:
+        G = core.group
+        bytes_launch = G * conn.n * (4 * 3 * 2 + 1 + 4) + G * conn.n * (core.max_block + 1) / 8
+        alg = bytes_launch
+        achieved = bytes_launch / (upd_ms / 1000.0) / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "traffic": NCU_TRAFFIC_PER_LAUNCH,
+                "kernel": "k_update", "launch_ms": upd_ms,
+                "algorithmic_bytes_per_launch": alg, "peak_kind": peak_kind}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        sample_steps = 10
+        dt = cpu_sample(conn, specs, sample_steps, threads)
+        cpu = {"value": args.trials * conn.n * sample_steps / dt, "unit": "neuron-steps/s",
+               "cores": threads, "kind": "port",
+               "sample": "%d trials x %d steps, csrmv over all edges (the reference's default "
+                         "CPU path), C port in oracle/" % (args.trials, sample_steps)}
+
+    if rank == 0:
+        line = {
+            "metric": "batched neuron-steps/s", "value": value, "unit": "neuron-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "trials_per_gpu": args.trials,
+                       "sim_steps": args.sim_steps, "trial_group": core.group,
+                       "block_steps": core.max_block,
+                       "l2": "inputs larger than L2 (trial state 150 MB, spike lists "
+                             "%.0f MB, CSR 60 MB)" % (core.lists.numel() * 4 / 1e6),
+                       "parallelism": "replicas x%d" % world},
+            "clocks": clocks,
+            "e2e": {"value": e2e, "unit": "neuron-steps/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": args.steps * blocks * core.launches_per_block(),
+            "roofline": roof,
+            "plain_1trial": plain,
+            "batched_over_plain": (value / world) / plain["value"] if plain else None,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -11,13 +11,18 @@ namespace fis {
 constexpr int kWarp = 32;
 
 // Philox4x32-10, the counter-based generator of Salmon, Moraes, Dror and
-// Shaw, "Parallel random numbers: as easy as 1, 2, 3" (SC'11).  Ten rounds of
-// two 32x32->64 multiplies; the key is bumped by the Weyl constants between
-// rounds.  Only the first output word is used: one Bernoulli draw per
-// (trial, step, neuron) counter.
-__host__ __device__ __forceinline__ uint32_t philox_x0(uint32_t c0, uint32_t c1,
-                                                       uint32_t c2, uint32_t c3,
-                                                       uint32_t k0, uint32_t k1) {
+// Shaw, "Parallel random numbers: as easy as 1, 2, 3" (SC'11): ten rounds of
+// two 32x32->64 multiplies, the key bumped by the Weyl constants between
+// rounds.
+// All four output words of Philox4x32-10.  The drive uses one call per four
+// steps of a neuron: counter (neuron, own_step / 4 low, own_step / 4 high,
+// trial lane), word own_step % 4 is the draw of that step.
+struct Philox4 {
+  uint32_t x[4];
+};
+
+__host__ __device__ __forceinline__ Philox4 philox4(uint32_t c0, uint32_t c1, uint32_t c2,
+                                                    uint32_t c3, uint32_t k0, uint32_t k1) {
 #pragma unroll
   for (int r = 0; r < 10; ++r) {
     if (r) {
@@ -40,7 +45,12 @@ __host__ __device__ __forceinline__ uint32_t philox_x0(uint32_t c0, uint32_t c1,
     c2 = n2;
     c3 = lo0;
   }
-  return c0;
+  Philox4 r;
+  r.x[0] = c0;
+  r.x[1] = c1;
+  r.x[2] = c2;
+  r.x[3] = c3;
+  return r;
 }
 
 // Packed edge: postsynaptic index in the high 18 bits, signed count low 14.

@@ -42,6 +42,16 @@ constexpr int kScatThreads = 256;
 constexpr int kScatWarps = kScatThreads / kWarp;
 constexpr int kMaxLists = 11264;  // prefix entries in dynamic shared memory (44 KB)
 
+// 4-byte asynchronous global -> shared copy (sm_80+ cp.async), completed by
+// cp_async_wait_all() in the issuing thread.
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
 int sm_count() {
   static int cached[64] = {0};
   int dev = 0;
@@ -190,43 +200,47 @@ k_scatter(const fis_engine E, const ScatterArgs A) {
 // phase B: K fused steps per neuron
 // ---------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(kUpdThreads)
+__global__ void __launch_bounds__(kUpdThreads, 4)
 k_update(const fis_engine E, const int b0, const int nb, const int K,
          int32_t* __restrict__ ring, float* __restrict__ spikes_out,
          const int bump) {
+  // The block's delayed input, one column per thread: staged here so the step
+  // loop below stays rolled (a compact body that fits the instruction cache)
+  // and can index it by step.
+  __shared__ int32_t sring[FIS_MAX_BLOCK][kUpdThreads];
   const int n = E.n;
   const int B = E.batch;
   const int L = E.p.lag;
   const int Wd = (n + kWarp - 1) / kWarp;
-  const int64_t npad = (int64_t)Wd * kWarp;
-  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int npad = Wd * kWarp;
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;  // < 2**31, checked on the host
   const int64_t t0 = *E.clock;
 
-  if (gid < (int64_t)nb * npad) {
-    const int bl = (int)(gid / npad);
-    const int i = (int)(gid - (int64_t)bl * npad);
+  if (gid < nb * npad) {
+    const int bl = gid / npad;
+    const int i = gid - bl * npad;
     const int b = b0 + bl;
     const int word = i >> 5;
     const int lane = threadIdx.x & (kWarp - 1);
     const bool valid = i < n;
     const fis_trial tr = E.trials[b];
-    int64_t ka64 = tr.start - t0, kb64 = tr.end - t0;
-    const int ka = (int)max((int64_t)0, min(ka64, (int64_t)K));
-    const int kb = (int)max((int64_t)0, min(kb64, (int64_t)K));
+    const int ka = (int)max((int64_t)0, min(tr.start - t0, (int64_t)K));
+    const int kb = (int)max((int64_t)0, min(tr.end - t0, (int64_t)K));
 
-    // Delayed input of all K steps, loaded up front; consumed slots return to
-    // zero so the scratch ring needs no separate clearing pass.
-    int32_t c[FIS_MAX_BLOCK];
+    // Stage the delayed input of the K steps with asynchronous copies (no
+    // registers held, all K requests in flight at once).
     const int64_t sstride = (int64_t)nb * n;
     int32_t* rp = ring + (int64_t)bl * n + i;
-#pragma unroll
-    for (int k = 0; k < FIS_MAX_BLOCK; ++k) {
-      c[k] = 0;
-      if (k < K && valid) c[k] = rp[k * sstride];
+    {
+      const int32_t* src = rp;
+#pragma unroll 4
+      for (int k = 0; k < K; ++k) {
+        if (valid) cp_async4(&sring[k][threadIdx.x], src);
+        else sring[k][threadIdx.x] = 0;
+        src += sstride;
+      }
+      cp_async_wait_all();
     }
-#pragma unroll
-    for (int k = 0; k < FIS_MAX_BLOCK; ++k)
-      if (k < K && valid && c[k] != 0) rp[k * sstride] = 0;
 
     const int64_t sidx = (int64_t)b * n + i;
     float v = 0.f, g = 0.f, r = 0.f, rate = 0.f;
@@ -238,9 +252,12 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
       fl = E.flags[sidx];
       rate = E.rates[sidx];
     }
+    int slot = (int)mod_pos(t0, L);        // ring-of-lists slot of the current step
+    int slot2 = (int)mod_pos(t0, 2 * L);   // list_len row of the current step
     bool s_prev = false;
     if (t0 - 1 >= tr.start && t0 >= 1) {
-      const uint32_t wv = E.bits[(mod_pos(t0 - 1, L) * B + b) * Wd + word];
+      const int sp = slot == 0 ? L - 1 : slot - 1;
+      const uint32_t wv = E.bits[((int64_t)sp * B + b) * Wd + word];
       s_prev = (wv >> lane) & 1u;
     }
     const float m_fire = (fl & FIS_FL_FIRE_OFF) ? 0.f : 1.f;
@@ -254,60 +271,80 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
     const float prob = __fmul_rn(rate, E.p.prob_scale);
     const bool driven = prob > 0.f;
     const uint32_t key0 = (uint32_t)tr.seed, key1 = (uint32_t)(tr.seed >> 32);
+    const int64_t own0 = t0 - tr.start;  // the trial's own step at k = 0
+    uint32_t rw0 = 0, rw1 = 0, rw2 = 0, rw3 = 0;
+    bool have_rw = false;
+    const int64_t bstride = (int64_t)B * Wd;
+    uint32_t* bitp = E.bits + (int64_t)slot * bstride + (int64_t)b * Wd + word;
 
-#pragma unroll
-    for (int k = 0; k < FIS_MAX_BLOCK; ++k) {
-      if (k < K) {
-        const int64_t u = t0 + k;
-        bool fired = false;
-        if (valid && k >= ka && k < kb) {
-          // refractory counter and gate (sim.py:921-923)
-          const float s = s_prev ? 1.f : 0.f;
-          r = __fmul_rn(__fadd_rn(r, 1.f), __fsub_rn(1.f, s));
-          const float gate = (r >= rs) ? 1.f : 0.f;
-          // delayed input and the new conductance (sim.py:928-929)
-          const int32_t ck = silenced ? 0 : c[k];
-          const float delayed = __fmul_rn(__fmul_rn(E.p.w_scale, __int2float_rn(ck)), m_in);
-          const float gn = __fadd_rn(__fmul_rn(g, E.p.a_syn), __fmul_rn(delayed, gate));
-          // Poisson drive (sim.py:859-861): one Philox word per draw
-          float vstim = 0.f;
-          if (E.vstim) {
-            vstim = E.vstim[sidx];
-          } else if (driven) {
-            const int64_t own = u - tr.start;
-            const uint32_t x = philox_x0((uint32_t)i, (uint32_t)own,
-                                         (uint32_t)((uint64_t)own >> 32), tr.stream,
-                                         key0, key1);
-            if (__fmul_rn((float)(x >> 8), 0x1p-24f) < prob) vstim = E.p.kick;
+#pragma unroll 1
+    for (int k = 0; k < K; ++k) {
+      bool fired = false;
+      // consumed slots return to zero: the scratch ring needs no clearing pass
+      if (valid && sring[k][threadIdx.x] != 0) *rp = 0;
+      rp += sstride;
+      if (valid && k >= ka && k < kb) {
+        // refractory counter and gate (sim.py:921-923)
+        const float s = s_prev ? 1.f : 0.f;
+        r = __fmul_rn(__fadd_rn(r, 1.f), __fsub_rn(1.f, s));
+        const float gate = (r >= rs) ? 1.f : 0.f;
+        // delayed input and the new conductance (sim.py:928-929)
+        const int32_t ck = silenced ? 0 : sring[k][threadIdx.x];
+        const float delayed = __fmul_rn(__fmul_rn(E.p.w_scale, __int2float_rn(ck)), m_in);
+        const float gn = __fadd_rn(__fmul_rn(g, E.p.a_syn), __fmul_rn(delayed, gate));
+        // Poisson drive (sim.py:859-861)
+        float vstim = 0.f;
+        if (E.vstim) {
+          vstim = E.vstim[sidx];
+        } else if (driven) {
+          const int64_t own = own0 + k;
+          const int q = (int)(own & 3);
+          if (!have_rw || q == 0) {
+            const uint64_t quad = (uint64_t)own >> 2;
+            const Philox4 r4 = philox4((uint32_t)i, (uint32_t)quad, (uint32_t)(quad >> 32),
+                                       tr.stream, key0, key1);
+            rw0 = r4.x[0];
+            rw1 = r4.x[1];
+            rw2 = r4.x[2];
+            rw3 = r4.x[3];
+            have_rw = true;
           }
-          // membrane with the previous conductance (sim.py:936-938)
-          v = __fadd_rn(v, vstim);
-          v = __fadd_rn(v, __fmul_rn(E.p.a_mem, __fsub_rn(g, __fsub_rn(v, E.p.v_rest))));
-          // hold, threshold, reset (sim.py:943-952)
-          v = __fadd_rn(__fmul_rn(v, m_hold), v_hold);
-          const float sp = __fmul_rn((v > E.p.v_th) ? 1.f : 0.f, m_fire);
-          v = __fsub_rn(v, __fmul_rn(__fsub_rn(v, E.p.v_reset), sp));
-          g = __fsub_rn(gn, __fmul_rn(gn, sp));
-          fired = sp != 0.f;
-          s_prev = fired;
+          const uint32_t x = q == 0 ? rw0 : q == 1 ? rw1 : q == 2 ? rw2 : rw3;
+          if (__fmul_rn((float)(x >> 8), 0x1p-24f) < prob) vstim = E.p.kick;
         }
-        const unsigned bal = __ballot_sync(0xFFFFFFFFu, fired);
-        if (lane == 0) E.bits[(mod_pos(u, L) * B + b) * Wd + word] = bal;
-        if (fired) {
-          const int nch = E.nchunks[i];
-          if ((out_on || k == K - 1) && nch > 0) {
-            int32_t* lenp = E.list_len + mod_pos(u, 2 * L) * B + b;
-            const int32_t pos = atomicAdd(lenp, nch);
-            uint32_t* dst = E.lists + ((int64_t)mod_pos(u, L) * B + b) * E.list_cap;
-            for (int q = 0; q < nch; ++q)
-              if (pos + q < E.list_cap) dst[pos + q] = ((uint32_t)i << 8) | (uint32_t)q;
-          }
-          if (tr.rec >= 0 && tr.rec < E.n_recs && tr.bin_steps > 0) {
-            const int64_t bin = (u - tr.start) / tr.bin_steps;
-            if (bin < tr.n_bins) atomicAdd(E.recs[tr.rec] + bin * n + i, 1);
-          }
+        // membrane with the previous conductance (sim.py:936-938)
+        v = __fadd_rn(v, vstim);
+        v = __fadd_rn(v, __fmul_rn(E.p.a_mem, __fsub_rn(g, __fsub_rn(v, E.p.v_rest))));
+        // hold, threshold, reset (sim.py:943-952)
+        v = __fadd_rn(__fmul_rn(v, m_hold), v_hold);
+        const float sp = __fmul_rn((v > E.p.v_th) ? 1.f : 0.f, m_fire);
+        v = __fsub_rn(v, __fmul_rn(__fsub_rn(v, E.p.v_reset), sp));
+        g = __fsub_rn(gn, __fmul_rn(gn, sp));
+        fired = sp != 0.f;
+        s_prev = fired;
+      }
+      const unsigned bal = __ballot_sync(0xFFFFFFFFu, fired);
+      if (lane == 0) *bitp = bal;
+      if (fired) {
+        const int nch = E.nchunks[i];
+        if ((out_on || k == K - 1) && nch > 0) {
+          const int32_t pos = atomicAdd(E.list_len + (int64_t)slot2 * B + b, nch);
+          uint32_t* dst = E.lists + ((int64_t)slot * B + b) * E.list_cap;
+          for (int q = 0; q < nch; ++q)
+            if (pos + q < E.list_cap) dst[pos + q] = ((uint32_t)i << 8) | (uint32_t)q;
+        }
+        if (tr.rec >= 0 && tr.rec < E.n_recs && tr.bin_steps > 0) {
+          const int64_t bin = (own0 + k) / tr.bin_steps;
+          if (bin < tr.n_bins) atomicAdd(E.recs[tr.rec] + bin * n + i, 1);
         }
       }
+      if (++slot == L) {
+        slot = 0;
+        bitp -= (int64_t)(L - 1) * bstride;
+      } else {
+        bitp += bstride;
+      }
+      if (++slot2 == 2 * L) slot2 = 0;
     }
     if (valid && ka < kb) {
       E.v[sidx] = v;
@@ -447,40 +484,88 @@ int fis_check(const fis_engine* e) {
   return FIS_OK;
 }
 
-int fis_block(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps,
-              int32_t* ring, float* spikes_out, int32_t last_group, void* stream) {
+static int check_block(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps,
+                       const int32_t* ring) {
   int rc = fis_check(e);
   if (rc) return rc;
   if ((rc = check_range(e, b0, nb))) return rc;
   if (!ring) return FIS_E_ARG;
-  const int L = e->p.lag;
-  if (k_steps < 1 || k_steps > FIS_MAX_BLOCK || k_steps > L) return FIS_E_BOUNDS;
+  if (k_steps < 1 || k_steps > FIS_MAX_BLOCK || k_steps > e->p.lag) return FIS_E_BOUNDS;
   if (e->vstim && k_steps != 1) return FIS_E_BOUNDS;
-  const int nlists = (k_steps + 1) * nb;
-  if (nlists + 1 > kMaxLists) return FIS_E_BOUNDS;
-  cudaStream_t st = (cudaStream_t)stream;
+  if ((k_steps + 1) * nb + 1 > kMaxLists) return FIS_E_BOUNDS;
+  const int64_t threads = (int64_t)nb * ((e->n + kWarp - 1) / kWarp) * kWarp;
+  if (threads + kUpdThreads > 0x7FFFFFFFLL) return FIS_E_BOUNDS;
+  return FIS_OK;
+}
 
+int fis_scatter(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, int32_t* ring,
+                void* stream) {
+  const int rc = check_block(e, b0, nb, k_steps, ring);
+  if (rc) return rc;
   ScatterArgs A;
   A.b0 = b0;
   A.nb = nb;
   A.nsrc = k_steps;
-  A.u_off = -(int64_t)L;
+  A.u_off = -(int64_t)e->p.lag;
   A.slot_mode = 0;
   A.zero_next = k_steps;
   A.filter_last = 1;
   A.ring = ring;
-  const size_t smem = sizeof(int32_t) * (size_t)(nlists + 1);
-  const int sgrid = sm_count() * 4;
-  k_scatter<<<sgrid, kScatThreads, smem, st>>>(*e, A);
-  if ((rc = launch_status())) return rc;
-
-  const int Wd = (e->n + kWarp - 1) / kWarp;
-  const int64_t threads = (int64_t)nb * Wd * kWarp;
-  const int64_t ugrid = (threads + kUpdThreads - 1) / kUpdThreads;
-  if (ugrid > 0x7FFFFFFF) return FIS_E_BOUNDS;
-  k_update<<<(unsigned)ugrid, kUpdThreads, 0, st>>>(*e, b0, nb, k_steps, ring, spikes_out,
-                                                    last_group ? 1 : 0);
+  const size_t smem = sizeof(int32_t) * (size_t)((k_steps + 1) * nb + 1);
+  k_scatter<<<sm_count() * 4, kScatThreads, smem, (cudaStream_t)stream>>>(*e, A);
   return launch_status();
+}
+
+int fis_update(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, int32_t* ring,
+               float* spikes_out, int32_t last_group, void* stream) {
+  const int rc = check_block(e, b0, nb, k_steps, ring);
+  if (rc) return rc;
+  const int64_t threads = (int64_t)nb * ((e->n + kWarp - 1) / kWarp) * kWarp;
+  const int64_t ugrid = (threads + kUpdThreads - 1) / kUpdThreads;
+  k_update<<<(unsigned)ugrid, kUpdThreads, 0, (cudaStream_t)stream>>>(
+      *e, b0, nb, k_steps, ring, spikes_out, last_group ? 1 : 0);
+  return launch_status();
+}
+
+int fis_block(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, int32_t* ring,
+              float* spikes_out, int32_t last_group, void* stream) {
+  const int rc = fis_scatter(e, b0, nb, k_steps, ring, stream);
+  if (rc) return rc;
+  return fis_update(e, b0, nb, k_steps, ring, spikes_out, last_group, stream);
+}
+
+int fis_advance(const fis_engine* e, int64_t steps, int32_t group, int32_t* ring,
+                float* spikes_out, void* const* events, int32_t n_pairs, int32_t every,
+                void* stream) {
+  int rc = fis_check(e);
+  if (rc) return rc;
+  if (steps < 0 || group < 1 || !ring) return FIS_E_ARG;
+  if (events && (n_pairs < 0 || every < 1)) return FIS_E_ARG;
+  const int kmax = e->p.lag < FIS_MAX_BLOCK ? e->p.lag : FIS_MAX_BLOCK;
+  cudaStream_t st = (cudaStream_t)stream;
+  int64_t left = steps;
+  int64_t launch = 0;
+  while (left > 0) {
+    const int k = (int)(left < kmax ? left : kmax);
+    float* sp = (left == k) ? spikes_out : nullptr;
+    for (int32_t g0 = 0; g0 < e->batch; g0 += group) {
+      const int32_t nb = (e->batch - g0) < group ? (e->batch - g0) : group;
+      if ((rc = fis_scatter(e, g0, nb, k, ring, stream))) return rc;
+      const bool timed = events && (launch % every) == 0 && (launch / every) < n_pairs;
+      if (timed) {
+        if ((rc = (int)cudaEventRecord((cudaEvent_t)events[2 * (launch / every)], st)))
+          return rc;
+      }
+      if ((rc = fis_update(e, g0, nb, k, ring, sp, g0 + nb == e->batch, stream))) return rc;
+      if (timed) {
+        if ((rc = (int)cudaEventRecord((cudaEvent_t)events[2 * (launch / every) + 1], st)))
+          return rc;
+      }
+      ++launch;
+    }
+    left -= k;
+  }
+  return FIS_OK;
 }
 
 int fis_delay_buffer(const fis_engine* e, int32_t b0, int32_t nb, int32_t* scratch,

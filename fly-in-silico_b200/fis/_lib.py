@@ -35,6 +35,7 @@ STATUS = {0: "ok", -1: "FIS_E_ARG (null pointer or size out of range)",
 # Every symbol include/fis.h declares, checked at load time and by the tests.
 EXPORTS = ("ev_spmv_i32", "ev_spmv_i64", "ev_spmv_abi", "fis_abi",
            "fis_sizeof_engine", "fis_sizeof_trial", "fis_check", "fis_block",
+           "fis_scatter", "fis_update", "fis_advance",
            "fis_delay_buffer", "fis_spikes_f32", "fis_load_spikes", "fis_add_rows")
 
 
@@ -99,13 +100,17 @@ def load(path=None):
         getattr(L, name).argtypes = []
     L.fis_check.argtypes = [P]
     L.fis_block.argtypes = [P, I32, I32, I32, P, P, I32, P]
+    L.fis_scatter.argtypes = [P, I32, I32, I32, P, P]
+    L.fis_advance.argtypes = [P, I64, I32, P, P, P, I32, I32, P]
+    L.fis_update.argtypes = [P, I32, I32, I32, P, P, I32, P]
     L.fis_delay_buffer.argtypes = [P, I32, I32, P, P, P]
     L.fis_spikes_f32.argtypes = [P, I32, I32, I64, P, P]
     L.fis_load_spikes.argtypes = [P, I32, I32, P, P]
     L.fis_add_rows.argtypes = [P, I32, I32, P, I64, P, I64, P]
     L.ev_spmv_i32.argtypes = [P, P, P, P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P]
     L.ev_spmv_i64.argtypes = [P, P, P, P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P]
-    for s in ("fis_check", "fis_block", "fis_delay_buffer", "fis_spikes_f32",
+    for s in ("fis_check", "fis_block", "fis_scatter", "fis_update", "fis_advance",
+              "fis_delay_buffer", "fis_spikes_f32",
               "fis_load_spikes", "fis_add_rows", "ev_spmv_i32", "ev_spmv_i64"):
         getattr(L, s).restype = ctypes.c_int
     if L.fis_abi() != FIS_ABI_VERSION:

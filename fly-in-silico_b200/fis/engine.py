@@ -221,8 +221,13 @@ class Core:
 
     # --- stepping ------------------------------------------------------------
 
-    def block(self, k, spikes_out=None, stream=None):
-        """Advance every slot by ``k`` steps (1 <= k <= max_block)."""
+    def block(self, k, spikes_out=None, stream=None, timer=None):
+        """Advance every slot by ``k`` steps (1 <= k <= max_block).
+
+        ``timer`` (optional) is called as ``timer(stream, True)`` right before
+        and ``timer(stream, False)`` right after each update launch, so a caller
+        can bracket the dominant kernel with CUDA events.
+        """
         k = int(k)
         if not 1 <= k <= self.max_block:
             raise ValueError("block of %d steps; 1..%d allowed" % (k, self.max_block))
@@ -234,10 +239,17 @@ class Core:
             nb = min(G, B - g0)
             if self.pending is not None:
                 self._apply_pending(g0, nb, k, st)
-            rc = self.lib.fis_block(ctypes.byref(self.desc), g0, nb, k,
-                                    ctypes.c_void_p(self.ring.data_ptr()), sp,
-                                    1 if g0 + nb == B else 0, ctypes.c_void_p(st))
-            _lib.check(rc, "fis_block")
+            ring = ctypes.c_void_p(self.ring.data_ptr())
+            rc = self.lib.fis_scatter(ctypes.byref(self.desc), g0, nb, k, ring,
+                                      ctypes.c_void_p(st))
+            _lib.check(rc, "fis_scatter")
+            if timer is not None:
+                timer(st, True)
+            rc = self.lib.fis_update(ctypes.byref(self.desc), g0, nb, k, ring, sp,
+                                     1 if g0 + nb == B else 0, ctypes.c_void_p(st))
+            _lib.check(rc, "fis_update")
+            if timer is not None:
+                timer(st, False)
         self.step += k
         if self.pending is not None and self.step >= self.pending[0] + self.buf_len:
             self.pending = None
@@ -257,13 +269,43 @@ class Core:
                                    nb * n, ctypes.c_void_p(st))
         _lib.check(rc, "fis_add_rows")
 
-    def advance(self, steps, spikes_out=None):
-        """``steps`` steps in blocks of at most ``max_block``."""
-        left = int(steps)
-        while left > 0:
-            k = min(left, self.max_block)
-            self.block(k, spikes_out=spikes_out if k == left else None)
-            left -= k
+    def advance(self, steps, spikes_out=None, timer=None, events=None, every=1):
+        """``steps`` steps in blocks of at most ``max_block``.
+
+        Runs the native block loop ``fis_advance`` unless restored pending
+        input or a Python ``timer`` needs the per-block path.  ``events``: a
+        list of ``torch.cuda.Event`` pairs (flattened) recorded around every
+        ``every``-th update launch.
+        """
+        steps = int(steps)
+        if steps <= 0:
+            return
+        if self.pending is not None or timer is not None or self.max_block != min(
+                _lib.FIS_MAX_BLOCK, self.lag):
+            left = steps
+            while left > 0:
+                k = min(left, self.max_block)
+                self.block(k, spikes_out=spikes_out if k == left else None, timer=timer)
+                left -= k
+            return
+        self._sync_trials()
+        st = torch.cuda.current_stream(self.device)
+        ev_arr, n_pairs = None, 0
+        if events:
+            for e in events:  # materialize the event handles on this stream
+                e.record(st)
+            n_pairs = len(events) // 2
+            ev_arr = (ctypes.c_void_p * (2 * n_pairs))(*[e.cuda_event for e in events[:2 * n_pairs]])
+        rc = self.lib.fis_advance(ctypes.byref(self.desc), steps, self.group,
+                                  ctypes.c_void_p(self.ring.data_ptr()),
+                                  ctypes.c_void_p(spikes_out.data_ptr()) if spikes_out is not None else None,
+                                  ev_arr, n_pairs, max(1, int(every)), ctypes.c_void_p(st.cuda_stream))
+        _lib.check(rc, "fis_advance")
+        self.step += steps
+
+    def launches_per_block(self):
+        """Kernel launches of one block (scatter + update per trial group)."""
+        return 2 * (-(-self.batch // self.group))
 
     # --- readouts -------------------------------------------------------------
 

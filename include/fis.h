@@ -179,6 +179,29 @@ int fis_block(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps,
               int32_t* ring, float* spikes_out, int32_t last_group,
               void* stream);
 
+/* Phase A of fis_block alone: the scatter into `ring` (same arguments). */
+int fis_scatter(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps,
+                int32_t* ring, void* stream);
+
+/* Phase B of fis_block alone: the fused update draining `ring`. */
+int fis_update(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps,
+               int32_t* ring, float* spikes_out, int32_t last_group, void* stream);
+
+/*
+ * Advance every slot by `steps` steps: blocks of min(FIS_MAX_BLOCK, lag)
+ * steps (the last one shorter), each block running fis_scatter + fis_update
+ * for the trial groups [g0, g0+group) in turn.  The native form of a host
+ * loop over fis_block.
+ *   ring        int32 [min(FIS_MAX_BLOCK, lag)][group][N], zero on entry
+ *   spikes_out  float [B][N] or NULL, written by the last block
+ *   events      NULL, or 2*n_pairs cudaEvent_t handles: pair j is recorded
+ *               around the update launch number j*every (0-based over the
+ *               whole call), for timing the dominant kernel
+ */
+int fis_advance(const fis_engine* e, int64_t steps, int32_t group, int32_t* ring,
+                float* spikes_out, void* const* events, int32_t n_pairs,
+                int32_t every, void* stream);
+
 /*
  * Write the reference's pending delay ring (Engine.delay_buffer,
  * sim.py:385) for slots [b0, b0+nb): out float [nb][buf_len][N], slot

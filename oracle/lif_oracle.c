@@ -80,13 +80,16 @@ void oracle_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t
   memcpy(out, c, sizeof(c));
 }
 
-static uint32_t philox_x0(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
-                          uint64_t seed) {
-  const uint32_t ctr[4] = {c0, c1, c2, c3};
+/* The draw of neuron i at own step `own`: Philox4x32-10 with counter
+ * (i, own/4 low, own/4 high, stream) and key (seed low, seed high); word
+ * own % 4 of the output. */
+static uint32_t drive_word(int i, int64_t own, uint32_t stream, uint64_t seed) {
+  const uint64_t quad = (uint64_t)own >> 2;
+  const uint32_t ctr[4] = {(uint32_t)i, (uint32_t)quad, (uint32_t)(quad >> 32), stream};
   const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
   uint32_t out[4];
   oracle_philox4x32_10(ctr, key, out);
-  return out[0];
+  return out[own & 3];
 }
 
 /* One draw: fire iff float(x >> 8) * 2**-24 < f32(rate) * f32(dt/1000). */
@@ -94,8 +97,7 @@ static float drive_one(float rate, float prob_scale, float kick, int i, int64_t 
                        uint64_t seed, uint32_t stream) {
   const float p = rate * prob_scale;
   if (!(p > 0.0f)) return 0.0f * kick; /* the reference's w * (0 * gain) */
-  const uint32_t x = philox_x0((uint32_t)i, (uint32_t)own, (uint32_t)((uint64_t)own >> 32),
-                               stream, seed);
+  const uint32_t x = drive_word(i, own, stream, seed);
   const float u = (float)(x >> 8) * 0x1p-24f;
   return (u < p) ? kick : 0.0f * kick;
 }
