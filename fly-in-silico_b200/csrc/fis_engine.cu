@@ -200,6 +200,39 @@ k_scatter(const fis_engine E, const ScatterArgs A) {
 // phase B: K fused steps per neuron
 // ---------------------------------------------------------------------------
 
+// One neuron's state for the step loop.
+struct Neuron {
+  float v, g, r;      // membrane, conductance, refractory counter
+  float keep;         // 1 - spike of the previous step
+  float m_fire, m_in, m_hold, v_hold, rs;
+  bool silenced;
+};
+
+// One step of sim.py:921-952 for one neuron, the reference's operation order
+// one rounding at a time.  Returns the spike (0 or 1).
+__device__ __forceinline__ float lif_step(Neuron& s, const fis_lif_params& P, int32_t c_in,
+                                          float vstim) {
+  // refractory counter and gate (sim.py:921-923)
+  s.r = __fmul_rn(__fadd_rn(s.r, 1.f), s.keep);
+  const float gate = (s.r >= s.rs) ? 1.f : 0.f;
+  // delayed input and the new conductance (sim.py:928-929); a silenced neuron
+  // has no incoming synapses (sim.py:324-336)
+  const int32_t ck = s.silenced ? 0 : c_in;
+  const float delayed = __fmul_rn(__fmul_rn(P.w_scale, __int2float_rn(ck)), s.m_in);
+  const float gn = __fadd_rn(__fmul_rn(s.g, P.a_syn), __fmul_rn(delayed, gate));
+  // membrane with the previous conductance (sim.py:936-938)
+  float v = __fadd_rn(s.v, vstim);
+  v = __fadd_rn(v, __fmul_rn(P.a_mem, __fsub_rn(s.g, __fsub_rn(v, P.v_rest))));
+  // hold, threshold, reset (sim.py:943-952)
+  v = __fadd_rn(__fmul_rn(v, s.m_hold), s.v_hold);
+  const float sp = __fmul_rn((v > P.v_th) ? 1.f : 0.f, s.m_fire);
+  s.v = __fsub_rn(v, __fmul_rn(__fsub_rn(v, P.v_reset), sp));
+  s.g = __fsub_rn(gn, __fmul_rn(gn, sp));
+  s.keep = __fsub_rn(1.f, sp);
+  return sp;
+}
+
+template <bool kTape>
 __global__ void __launch_bounds__(kUpdThreads, 4)
 k_update(const fis_engine E, const int b0, const int nb, const int K,
          int32_t* __restrict__ ring, float* __restrict__ spikes_out,
@@ -208,8 +241,10 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
   // loop below stays rolled (a compact body that fits the instruction cache)
   // and can index it by step.
   __shared__ int32_t sring[FIS_MAX_BLOCK][kUpdThreads];
+  __shared__ uint32_t sdrive[kUpdThreads];                        // kick bit per step
+  __shared__ float sprob[kUpdThreads];                            // Bernoulli p per lane
+  __shared__ uint32_t sbal[kUpdThreads / kWarp][FIS_MAX_BLOCK];   // raster words per step
   const int n = E.n;
-  const int B = E.batch;
   const int L = E.p.lag;
   const int Wd = (n + kWarp - 1) / kWarp;
   const int npad = Wd * kWarp;
@@ -220,8 +255,8 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
     const int bl = gid / npad;
     const int i = gid - bl * npad;
     const int b = b0 + bl;
-    const int word = i >> 5;
     const int lane = threadIdx.x & (kWarp - 1);
+    const int wib = threadIdx.x / kWarp;
     const bool valid = i < n;
     const fis_trial tr = E.trials[b];
     const int ka = (int)max((int64_t)0, min(tr.start - t0, (int64_t)K));
@@ -229,7 +264,7 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
 
     // Stage the delayed input of the K steps with asynchronous copies (no
     // registers held, all K requests in flight at once).
-    const int64_t sstride = (int64_t)nb * n;
+    const int sstride = nb * n;  // < 2**31 / FIS_MAX_BLOCK, checked on the host
     int32_t* rp = ring + (int64_t)bl * n + i;
     {
       const int32_t* src = rp;
@@ -239,97 +274,143 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
         else sring[k][threadIdx.x] = 0;
         src += sstride;
       }
-      cp_async_wait_all();
     }
 
     const int64_t sidx = (int64_t)b * n + i;
-    float v = 0.f, g = 0.f, r = 0.f, rate = 0.f;
+    Neuron st;
+    float rate = 0.f;
     uint32_t fl = 0;
+    st.v = st.g = st.r = 0.f;
     if (valid && ka < kb) {
-      v = E.v[sidx];
-      g = E.g[sidx];
-      r = E.refrac[sidx];
+      st.v = E.v[sidx];
+      st.g = E.g[sidx];
+      st.r = E.refrac[sidx];
       fl = E.flags[sidx];
       rate = E.rates[sidx];
     }
-    int slot = (int)mod_pos(t0, L);        // ring-of-lists slot of the current step
-    int slot2 = (int)mod_pos(t0, 2 * L);   // list_len row of the current step
+    const int slot0 = (int)mod_pos(t0, L);  // ring-of-lists slot of step t0
+    // this warp's raster words, one per slot: bits[b][word][slot]
+    uint32_t* bitrow = E.bits + ((int64_t)b * Wd + (i >> 5)) * L;
     bool s_prev = false;
-    if (t0 - 1 >= tr.start && t0 >= 1) {
-      const int sp = slot == 0 ? L - 1 : slot - 1;
-      const uint32_t wv = E.bits[((int64_t)sp * B + b) * Wd + word];
-      s_prev = (wv >> lane) & 1u;
-    }
-    const float m_fire = (fl & FIS_FL_FIRE_OFF) ? 0.f : 1.f;
-    const bool out_on = !(fl & (FIS_FL_OUT_OFF | FIS_FL_SILENCED));
-    const bool silenced = fl & FIS_FL_SILENCED;
-    const float m_in = (fl & FIS_FL_IN_OFF) ? 0.f : 1.f;
+    if (t0 - 1 >= tr.start && t0 >= 1)
+      s_prev = (bitrow[slot0 == 0 ? L - 1 : slot0 - 1] >> lane) & 1u;
+    st.keep = s_prev ? 0.f : 1.f;
+    st.m_fire = (fl & FIS_FL_FIRE_OFF) ? 0.f : 1.f;
+    st.silenced = fl & FIS_FL_SILENCED;
+    st.m_in = (fl & FIS_FL_IN_OFF) ? 0.f : 1.f;
     const bool hold = fl & FIS_FL_HOLD;
-    const float m_hold = hold ? 0.f : 1.f;
-    const float v_hold = hold ? tr.v_clamp : 0.f;
-    const float rs = (fl & FIS_FL_NOREFRAC) ? 0.f : E.p.refrac_steps;
-    const float prob = __fmul_rn(rate, E.p.prob_scale);
-    const bool driven = prob > 0.f;
-    const uint32_t key0 = (uint32_t)tr.seed, key1 = (uint32_t)(tr.seed >> 32);
+    st.m_hold = hold ? 0.f : 1.f;
+    st.v_hold = hold ? tr.v_clamp : 0.f;
+    st.rs = (fl & FIS_FL_NOREFRAC) ? 0.f : E.p.refrac_steps;
     const int64_t own0 = t0 - tr.start;  // the trial's own step at k = 0
-    uint32_t rw0 = 0, rw1 = 0, rw2 = 0, rw3 = 0;
-    bool have_rw = false;
-    const int64_t bstride = (int64_t)B * Wd;
-    uint32_t* bitp = E.bits + (int64_t)slot * bstride + (int64_t)b * Wd + word;
 
-#pragma unroll 1
-    for (int k = 0; k < K; ++k) {
-      bool fired = false;
-      // consumed slots return to zero: the scratch ring needs no clearing pass
-      if (valid && sring[k][threadIdx.x] != 0) *rp = 0;
-      rp += sstride;
-      if (valid && k >= ka && k < kb) {
-        // refractory counter and gate (sim.py:921-923)
-        const float s = s_prev ? 1.f : 0.f;
-        r = __fmul_rn(__fadd_rn(r, 1.f), __fsub_rn(1.f, s));
-        const float gate = (r >= rs) ? 1.f : 0.f;
-        // delayed input and the new conductance (sim.py:928-929)
-        const int32_t ck = silenced ? 0 : sring[k][threadIdx.x];
-        const float delayed = __fmul_rn(__fmul_rn(E.p.w_scale, __int2float_rn(ck)), m_in);
-        const float gn = __fadd_rn(__fmul_rn(g, E.p.a_syn), __fmul_rn(delayed, gate));
-        // Poisson drive (sim.py:859-861)
-        float vstim = 0.f;
-        if (E.vstim) {
-          vstim = E.vstim[sidx];
-        } else if (driven) {
-          const int64_t own = own0 + k;
-          const int q = (int)(own & 3);
-          if (!have_rw || q == 0) {
-            const uint64_t quad = (uint64_t)own >> 2;
-            const Philox4 r4 = philox4((uint32_t)i, (uint32_t)quad, (uint32_t)(quad >> 32),
-                                       tr.stream, key0, key1);
-            rw0 = r4.x[0];
-            rw1 = r4.x[1];
-            rw2 = r4.x[2];
-            rw3 = r4.x[3];
-            have_rw = true;
+    // Poisson drive of the whole block (sim.py:859-861), before the step loop:
+    // draw j of neuron i is word j % 4 of Philox4x32-10 at counter
+    // (i, j / 4, trial lane); the (neuron, quad) pairs of the warp's driven
+    // neurons are spread over all 32 lanes, and each pair ORs its kick bits
+    // into the neuron's mask.
+    uint32_t dmask = 0;
+    if (!kTape) {
+      const float prob = __fmul_rn(rate, E.p.prob_scale);
+      const unsigned D = __ballot_sync(0xFFFFFFFFu, valid && ka < kb && prob > 0.f);
+      if (D) {
+        sdrive[threadIdx.x] = 0u;
+        sprob[threadIdx.x] = prob;
+        __syncwarp();
+        const int64_t own_a = own0 + ka;
+        const int64_t q0 = own_a >> 2;
+        const int nq = (int)(((own0 + kb - 1) >> 2) - q0) + 1;
+        const int total = __popc(D) * nq;
+        const int wbase = threadIdx.x - lane;
+        for (int it = lane; it < total; it += kWarp) {
+          const int jd = it / nq, qq = it - jd * nq;
+          unsigned m = D;
+          for (int t = 0; t < jd; ++t) m &= m - 1;
+          const int j = __ffs(m) - 1;
+          const int64_t quad = q0 + qq;
+          const Philox4 r4 = philox4((uint32_t)(i - lane + j), (uint32_t)quad,
+                                     (uint32_t)((uint64_t)quad >> 32), tr.stream,
+                                     (uint32_t)tr.seed, (uint32_t)(tr.seed >> 32));
+          const float pj = sprob[wbase + j];
+          uint32_t bits = 0;
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int k = (int)(quad * 4 + q - own0);
+            if (k >= ka && k < kb && __fmul_rn((float)(r4.x[q] >> 8), 0x1p-24f) < pj)
+              bits |= 1u << k;
           }
-          const uint32_t x = q == 0 ? rw0 : q == 1 ? rw1 : q == 2 ? rw2 : rw3;
-          if (__fmul_rn((float)(x >> 8), 0x1p-24f) < prob) vstim = E.p.kick;
+          if (bits) atomicOr(&sdrive[wbase + j], bits);
         }
-        // membrane with the previous conductance (sim.py:936-938)
-        v = __fadd_rn(v, vstim);
-        v = __fadd_rn(v, __fmul_rn(E.p.a_mem, __fsub_rn(g, __fsub_rn(v, E.p.v_rest))));
-        // hold, threshold, reset (sim.py:943-952)
-        v = __fadd_rn(__fmul_rn(v, m_hold), v_hold);
-        const float sp = __fmul_rn((v > E.p.v_th) ? 1.f : 0.f, m_fire);
-        v = __fsub_rn(v, __fmul_rn(__fsub_rn(v, E.p.v_reset), sp));
-        g = __fsub_rn(gn, __fmul_rn(gn, sp));
-        fired = sp != 0.f;
-        s_prev = fired;
+        __syncwarp();
+        dmask = sdrive[threadIdx.x];
       }
-      const unsigned bal = __ballot_sync(0xFFFFFFFFu, fired);
-      if (lane == 0) *bitp = bal;
-      if (fired) {
-        const int nch = E.nchunks[i];
+    }
+    cp_async_wait_all();
+
+    const float kick = E.p.kick;
+    uint32_t fired_mask = 0;
+    // Both loops are entered by whole warps (ka, kb depend on the trial only),
+    // so every lane reaches each ballot; lanes past the last neuron (valid is
+    // false) hold zero input and skip the update.
+    if (ka == 0 && kb == K) {
+      // the whole block is inside the trial: the plain loop
+#pragma unroll 1
+      for (int k = 0; k < K; ++k) {
+        const int32_t c_in = sring[k][threadIdx.x];
+        // consumed slots return to zero: the scratch ring needs no clearing pass
+        if (c_in != 0) rp[k * sstride] = 0;
+        float sp = 0.f;
+        if (valid) {
+          const float vstim = kTape ? E.vstim[sidx] : (((dmask >> k) & 1u) ? kick : 0.f);
+          sp = lif_step(st, E.p, c_in, vstim);
+        }
+        const unsigned bal = __ballot_sync(0xFFFFFFFFu, sp != 0.f);
+        if (lane == 0) sbal[wib][k] = bal;
+        fired_mask |= (sp != 0.f ? 1u : 0u) << k;
+      }
+    } else {
+#pragma unroll 1
+      for (int k = 0; k < K; ++k) {
+        const int32_t c_in = sring[k][threadIdx.x];
+        if (valid && c_in != 0) rp[k * sstride] = 0;
+        float sp = 0.f;
+        if (valid && k >= ka && k < kb) {
+          const float vstim = kTape ? E.vstim[sidx] : (((dmask >> k) & 1u) ? kick : 0.f);
+          sp = lif_step(st, E.p, c_in, vstim);
+        }
+        const unsigned bal = __ballot_sync(0xFFFFFFFFu, sp != 0.f);
+        if (lane == 0) sbal[wib][k] = bal;
+        fired_mask |= (sp != 0.f ? 1u : 0u) << k;
+      }
+    }
+    __syncwarp();
+    // the raster words of the K steps into the ring of the last L steps
+    if (lane < K) {
+      const int sl = slot0 + lane < L ? slot0 + lane : slot0 + lane - L;
+      bitrow[sl] = sbal[wib][lane];
+    }
+
+    if (valid && ka < kb) {
+      E.v[sidx] = st.v;
+      E.g[sidx] = st.g;
+      E.refrac[sidx] = st.r;
+    }
+    if (spikes_out && valid) spikes_out[sidx] = (st.keep == 0.f) ? 1.f : 0.f;
+
+    // Spike lists and recording for the (rare) steps this neuron fired.
+    if (fired_mask) {
+      const int B = E.batch;
+      const bool out_on = !(fl & (FIS_FL_OUT_OFF | FIS_FL_SILENCED));
+      const int nch = E.nchunks[i];
+      const int slot20 = (int)mod_pos(t0, 2 * L);
+      while (fired_mask) {
+        const int k = __ffs(fired_mask) - 1;
+        fired_mask &= fired_mask - 1;
+        const int sl = slot0 + k < L ? slot0 + k : slot0 + k - L;
+        const int sl2 = slot20 + k < 2 * L ? slot20 + k : slot20 + k - 2 * L;
         if ((out_on || k == K - 1) && nch > 0) {
-          const int32_t pos = atomicAdd(E.list_len + (int64_t)slot2 * B + b, nch);
-          uint32_t* dst = E.lists + ((int64_t)slot * B + b) * E.list_cap;
+          const int32_t pos = atomicAdd(E.list_len + (int64_t)sl2 * B + b, nch);
+          uint32_t* dst = E.lists + ((int64_t)sl * B + b) * E.list_cap;
           for (int q = 0; q < nch; ++q)
             if (pos + q < E.list_cap) dst[pos + q] = ((uint32_t)i << 8) | (uint32_t)q;
         }
@@ -338,20 +419,7 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
           if (bin < tr.n_bins) atomicAdd(E.recs[tr.rec] + bin * n + i, 1);
         }
       }
-      if (++slot == L) {
-        slot = 0;
-        bitp -= (int64_t)(L - 1) * bstride;
-      } else {
-        bitp += bstride;
-      }
-      if (++slot2 == 2 * L) slot2 = 0;
     }
-    if (valid && ka < kb) {
-      E.v[sidx] = v;
-      E.g[sidx] = g;
-      E.refrac[sidx] = r;
-    }
-    if (spikes_out && valid) spikes_out[sidx] = s_prev ? 1.f : 0.f;
   }
 
   if (bump) {
@@ -398,7 +466,7 @@ __global__ void k_spikes_f32(const fis_engine E, int b0, int nb, int64_t step,
   for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < total;
        x += (int64_t)gridDim.x * blockDim.x) {
     const int bl = (int)(x / n), i = (int)(x % n);
-    const uint32_t wv = E.bits[(mod_pos(step, L) * B + b0 + bl) * Wd + (i >> 5)];
+    const uint32_t wv = E.bits[((int64_t)(b0 + bl) * Wd + (i >> 5)) * L + mod_pos(step, L)];
     out[x] = ((wv >> (i & 31)) & 1u) ? 1.f : 0.f;
   }
 }
@@ -416,7 +484,7 @@ __global__ void k_load_spikes(const fis_engine E, int b0, int nb,
   const int b = b0 + bl;
   const bool fired = i < n && sp[(int64_t)bl * n + i] != 0.f;
   const unsigned bal = __ballot_sync(0xFFFFFFFFu, fired);
-  if ((threadIdx.x & 31) == 0) E.bits[(mod_pos(u, L) * B + b) * Wd + (i >> 5)] = bal;
+  if ((threadIdx.x & 31) == 0) E.bits[((int64_t)b * Wd + (i >> 5)) * L + mod_pos(u, L)] = bal;
   if (fired) {
     const int nch = E.nchunks[i];
     if (nch > 0) {
@@ -495,6 +563,7 @@ static int check_block(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_st
   if ((k_steps + 1) * nb + 1 > kMaxLists) return FIS_E_BOUNDS;
   const int64_t threads = (int64_t)nb * ((e->n + kWarp - 1) / kWarp) * kWarp;
   if (threads + kUpdThreads > 0x7FFFFFFFLL) return FIS_E_BOUNDS;
+  if ((int64_t)nb * e->n * FIS_MAX_BLOCK > 0x7FFFFFFFLL) return FIS_E_BOUNDS;
   return FIS_OK;
 }
 
@@ -522,8 +591,12 @@ int fis_update(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, int
   if (rc) return rc;
   const int64_t threads = (int64_t)nb * ((e->n + kWarp - 1) / kWarp) * kWarp;
   const int64_t ugrid = (threads + kUpdThreads - 1) / kUpdThreads;
-  k_update<<<(unsigned)ugrid, kUpdThreads, 0, (cudaStream_t)stream>>>(
-      *e, b0, nb, k_steps, ring, spikes_out, last_group ? 1 : 0);
+  if (e->vstim)
+    k_update<true><<<(unsigned)ugrid, kUpdThreads, 0, (cudaStream_t)stream>>>(
+        *e, b0, nb, k_steps, ring, spikes_out, last_group ? 1 : 0);
+  else
+    k_update<false><<<(unsigned)ugrid, kUpdThreads, 0, (cudaStream_t)stream>>>(
+        *e, b0, nb, k_steps, ring, spikes_out, last_group ? 1 : 0);
   return launch_status();
 }
 

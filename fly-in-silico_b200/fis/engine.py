@@ -12,7 +12,7 @@ Layout in HBM (B slots, N neurons, L = lag = buf_len + 1 = 20 by default):
 * state, trial-major [B][N]: ``v, g, refrac`` float32, ``flags`` uint8,
   ``rates`` float32 -- read once and written once per block of up to 20 steps;
 * spike history: ``lists`` uint32 [L][B][cap], ``list_len`` int32 [2L][B],
-  ``bits`` uint32 [L][B][ceil(N/32)];
+  ``bits`` uint32 [B][ceil(N/32)][L];
 * scratch ring int32 [K][G][N] for one trial group of G slots, reused by every
   group: sized to stay resident in the 126 MB L2 between the scatter that fills
   it and the update that drains it.
@@ -132,7 +132,7 @@ class Core:
             self.lists = torch.zeros((L, B, self.list_cap), dtype=torch.int32, device=dev)
             self.list_len = torch.zeros((2 * L, B), dtype=torch.int32, device=dev)
             self.words = (n + 31) // 32
-            self.bits = torch.zeros((L, B, self.words), dtype=torch.int32, device=dev)
+            self.bits = torch.zeros((B, self.words, L), dtype=torch.int32, device=dev)
             self.clock = torch.zeros(1, dtype=torch.int64, device=dev)
             self.done = torch.zeros(1, dtype=torch.int32, device=dev)
         self.trials = (_lib.Trial * B)()

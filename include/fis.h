@@ -98,7 +98,7 @@ typedef struct fis_trial {
  *   trials   fis_trial [B]
  *   lists    uint32 [L][B][list_cap]  spike entries pre << 8 | chunk
  *   list_len int32 [2L][B]     entries per (step mod 2L, trial)
- *   bits     uint32 [L][B][W]  spike raster of the last L steps
+ *   bits     uint32 [B][W][L]  spike raster of the last L steps (slot innermost)
  *   clock    int64 [1]         global steps completed (device-side)
  *   done     uint32 [1]        block-completion counter, zero between calls
  *   recs     int32* [n_recs]   recording buffers [n_bins][N]

@@ -21,9 +21,9 @@ def raster_rows(core, first, last):
     """Bit rows [step][B][nbytes] of global steps first..last-1 from the engine."""
     nbytes = (core.n + 7) // 8
     out = []
-    bits = core.bits.cpu().numpy()
+    bits = core.bits.cpu().numpy()  # [B][W][L]
     for s in range(first, last):
-        row = bits[s % core.lag].view(np.uint8)[:, :nbytes]
+        row = np.ascontiguousarray(bits[:, :, s % core.lag]).view(np.uint8)[:, :nbytes]
         out.append(row.copy())
     return out
 
