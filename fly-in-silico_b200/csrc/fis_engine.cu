@@ -52,6 +52,30 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_all;\n" ::: "memory");
 }
 
+// Bulk asynchronous shared -> global copy (sm_90+ cp.async.bulk, the TMA
+// engine): both addresses 16-byte aligned, size a multiple of 16.
+__device__ __forceinline__ void bulk_store(void* gmem, const void* smem, unsigned bytes) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(gmem),
+               "r"(sa), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() {
+  asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_all() {
+  asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
+}
+// Order this thread's generic-proxy shared-memory writes before later
+// async-proxy (bulk copy) reads of them.
+__device__ __forceinline__ void fence_proxy_async_shared() {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+
+// Ring rows are padded per trial to a whole number of update tiles.
+constexpr int kTile = 256;
+__host__ __device__ __forceinline__ int ring_row(int n) { return (n + kTile - 1) / kTile * kTile; }
+
 int sm_count() {
   static int cached[64] = {0};
   int dev = 0;
@@ -84,7 +108,8 @@ struct ScatterArgs {
   int slot_mode;      // 0: slot kk; 1: the reference ring slot (u + 1) % buf_len
   int zero_next;      // zero list_len of steps clock .. clock+zero_next-1
   int filter_last;    // handle the list of step clock-1 as described above
-  int32_t* ring;      // slot stride nb*n, trial stride n
+  int32_t* ring;      // slot stride nb*trial_stride
+  int trial_stride;   // elements per trial row of `ring`
 };
 
 __global__ void __launch_bounds__(kScatThreads)
@@ -147,7 +172,7 @@ k_scatter(const fis_engine E, const ScatterArgs A) {
 
   const int lane = threadIdx.x & (kWarp - 1);
   const int warp = threadIdx.x / kWarp;
-  const int64_t slot_stride = (int64_t)A.nb * n;
+  const int64_t slot_stride = (int64_t)A.nb * A.trial_stride;
   for (int32_t w = blockIdx.x * kScatWarps + warp; w < total; w += gridDim.x * kScatWarps) {
     // list holding work item w: largest j with pre_sum[j] <= w
     int lo = 0, hi = nlists - 1;
@@ -179,7 +204,7 @@ k_scatter(const fis_engine E, const ScatterArgs A) {
     const int64_t hi_e = min(r1, lo_e + (int64_t)E.chunk);
     if (lo_e >= hi_e) continue;
     const int slot = A.slot_mode ? (int)mod_pos(u + 1, E.p.buf_len) : kk;
-    int32_t* dst = A.ring + slot * slot_stride + (int64_t)bl * n;
+    int32_t* dst = A.ring + slot * slot_stride + (int64_t)bl * A.trial_stride;
     // 16-byte vector loads: four edges per lane, 128 edges per warp pass.
     for (int64_t p = (lo_e & ~(int64_t)3) + 4 * lane; p < hi_e; p += 4 * kWarp) {
       const uint4 q = __ldg(reinterpret_cast<const uint4*>(E.edges + p));
@@ -232,195 +257,234 @@ __device__ __forceinline__ float lif_step(Neuron& s, const fis_lif_params& P, in
   return sp;
 }
 
+// The step loop over K steps: `kDrive` selects whether any lane of the warp is
+// driven, so warps without drive carry no drive logic at all.  Returns the
+// number of spikes of this neuron (exact in float).
+template <bool kTape, bool kDrive>
+__device__ __forceinline__ float step_loop(Neuron& st, const fis_engine& E, int K, int ka,
+                                           int kb, bool valid, uint32_t dmask,
+                                           const int32_t (*sring)[kUpdThreads],
+                                           uint32_t* sbal, int lane, int64_t sidx) {
+  const float kick = E.p.kick;
+  float nspk = 0.f;
+  if (ka == 0 && kb == K) {
+#pragma unroll 2
+    for (int k = 0; k < K; ++k) {
+      const int32_t c_in = sring[k][threadIdx.x];
+      float sp = 0.f;
+      if (valid) {
+        float vstim = 0.f;
+        if (kTape) vstim = E.vstim[sidx];
+        else if (kDrive) vstim = ((dmask >> k) & 1u) ? kick : 0.f;
+        sp = lif_step(st, E.p, c_in, vstim);
+      }
+      const unsigned bal = __ballot_sync(0xFFFFFFFFu, sp != 0.f);
+      if (lane == 0) sbal[k] = bal;
+      nspk = __fadd_rn(nspk, sp);
+    }
+  } else {
+#pragma unroll 1
+    for (int k = 0; k < K; ++k) {
+      const int32_t c_in = sring[k][threadIdx.x];
+      float sp = 0.f;
+      if (valid && k >= ka && k < kb) {
+        float vstim = 0.f;
+        if (kTape) vstim = E.vstim[sidx];
+        else if (kDrive) vstim = ((dmask >> k) & 1u) ? kick : 0.f;
+        sp = lif_step(st, E.p, c_in, vstim);
+      }
+      const unsigned bal = __ballot_sync(0xFFFFFFFFu, sp != 0.f);
+      if (lane == 0) sbal[k] = bal;
+      nspk = __fadd_rn(nspk, sp);
+    }
+  }
+  return nspk;
+}
+
+// Grid: one CTA per (trial of the group, tile of 256 neurons); the trial's
+// rows of the scratch ring are padded to ring_row(n), so each CTA's slice of
+// a ring slot is one aligned 1 KB line of the async bulk copy engine.
 template <bool kTape>
 __global__ void __launch_bounds__(kUpdThreads, 4)
 k_update(const fis_engine E, const int b0, const int nb, const int K,
          int32_t* __restrict__ ring, float* __restrict__ spikes_out,
          const int bump) {
   // The block's delayed input, one column per thread: staged here so the step
-  // loop below stays rolled (a compact body that fits the instruction cache)
-  // and can index it by step.
+  // loop stays rolled (a compact body that fits the instruction cache) and can
+  // index it by step.
   __shared__ int32_t sring[FIS_MAX_BLOCK][kUpdThreads];
-  __shared__ uint32_t sdrive[kUpdThreads];                        // kick bit per step
-  __shared__ float sprob[kUpdThreads];                            // Bernoulli p per lane
-  __shared__ uint32_t sbal[kUpdThreads / kWarp][FIS_MAX_BLOCK];   // raster words per step
+  __shared__ __align__(16) int32_t szero[kUpdThreads];             // source of the clearing
+  __shared__ uint32_t sdrive[kUpdThreads];                         // kick bit per step
+  __shared__ float sprob[kUpdThreads];                             // Bernoulli p per lane
+  __shared__ uint32_t sbal[kUpdThreads / kWarp][FIS_MAX_BLOCK];    // raster words per step
   const int n = E.n;
   const int L = E.p.lag;
   const int Wd = (n + kWarp - 1) / kWarp;
-  const int npad = Wd * kWarp;
-  const int gid = blockIdx.x * blockDim.x + threadIdx.x;  // < 2**31, checked on the host
+  const int NR = ring_row(n);
+  const int tiles = NR / kTile;
+  const int bl = blockIdx.x / tiles;
+  const int tile = blockIdx.x - bl * tiles;
+  const int i = tile * kTile + threadIdx.x;
+  const int b = b0 + bl;
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int wib = threadIdx.x / kWarp;
+  const bool valid = i < n;
+  const bool warp_valid = (i - lane) < n;
   const int64_t t0 = *E.clock;
+  const fis_trial tr = E.trials[b];
+  const int ka = (int)max((int64_t)0, min(tr.start - t0, (int64_t)K));
+  const int kb = (int)max((int64_t)0, min(tr.end - t0, (int64_t)K));
+  const int64_t sidx = (int64_t)b * n + i;
 
-  if (gid < nb * npad) {
-    const int bl = gid / npad;
-    const int i = gid - bl * npad;
-    const int b = b0 + bl;
-    const int lane = threadIdx.x & (kWarp - 1);
-    const int wib = threadIdx.x / kWarp;
-    const bool valid = i < n;
-    const fis_trial tr = E.trials[b];
-    const int ka = (int)max((int64_t)0, min(tr.start - t0, (int64_t)K));
-    const int kb = (int)max((int64_t)0, min(tr.end - t0, (int64_t)K));
+  uint32_t fl = 0;
+  float rate = 0.f;
+  Neuron st;
+  st.v = st.g = st.r = 0.f;
+  if (valid && ka < kb) {
+    st.v = E.v[sidx];
+    st.g = E.g[sidx];
+    st.r = E.refrac[sidx];
+    fl = E.flags[sidx];
+    rate = E.rates[sidx];
+  }
+  st.silenced = fl & FIS_FL_SILENCED;
 
-    // Stage the delayed input of the K steps with asynchronous copies (no
-    // registers held, all K requests in flight at once).
-    const int sstride = nb * n;  // < 2**31 / FIS_MAX_BLOCK, checked on the host
-    int32_t* rp = ring + (int64_t)bl * n + i;
-    {
-      const int32_t* src = rp;
+  // Stage the delayed input of the K steps with asynchronous copies (no
+  // registers held, all K requests in flight at once).  A silenced neuron has
+  // no incoming synapses (sim.py:324-336): it stages zeros.
+  const int sstride = nb * NR;  // < 2**31 / FIS_MAX_BLOCK, checked on the host
+  int32_t* rtile = ring + (int64_t)bl * NR + tile * kTile;
+  {
+    const int32_t* src = rtile + threadIdx.x;
+    const bool load = valid && !st.silenced;
 #pragma unroll 4
-      for (int k = 0; k < K; ++k) {
-        if (valid) cp_async4(&sring[k][threadIdx.x], src);
-        else sring[k][threadIdx.x] = 0;
-        src += sstride;
-      }
+    for (int k = 0; k < K; ++k) {
+      if (load) cp_async4(&sring[k][threadIdx.x], src);
+      else sring[k][threadIdx.x] = 0;
+      src += sstride;
     }
+  }
+  szero[threadIdx.x] = 0;
 
-    const int64_t sidx = (int64_t)b * n + i;
-    Neuron st;
-    float rate = 0.f;
-    uint32_t fl = 0;
-    st.v = st.g = st.r = 0.f;
-    if (valid && ka < kb) {
-      st.v = E.v[sidx];
-      st.g = E.g[sidx];
-      st.r = E.refrac[sidx];
-      fl = E.flags[sidx];
-      rate = E.rates[sidx];
-    }
-    const int slot0 = (int)mod_pos(t0, L);  // ring-of-lists slot of step t0
-    // this warp's raster words, one per slot: bits[b][word][slot]
-    uint32_t* bitrow = E.bits + ((int64_t)b * Wd + (i >> 5)) * L;
-    bool s_prev = false;
-    if (t0 - 1 >= tr.start && t0 >= 1)
-      s_prev = (bitrow[slot0 == 0 ? L - 1 : slot0 - 1] >> lane) & 1u;
-    st.keep = s_prev ? 0.f : 1.f;
-    st.m_fire = (fl & FIS_FL_FIRE_OFF) ? 0.f : 1.f;
-    st.silenced = fl & FIS_FL_SILENCED;
-    st.m_in = (fl & FIS_FL_IN_OFF) ? 0.f : 1.f;
-    const bool hold = fl & FIS_FL_HOLD;
-    st.m_hold = hold ? 0.f : 1.f;
-    st.v_hold = hold ? tr.v_clamp : 0.f;
-    st.rs = (fl & FIS_FL_NOREFRAC) ? 0.f : E.p.refrac_steps;
-    const int64_t own0 = t0 - tr.start;  // the trial's own step at k = 0
+  const int slot0 = (int)mod_pos(t0, L);  // ring-of-lists slot of step t0
+  // this warp's raster words, one per slot: bits[b][word][slot]
+  uint32_t* bitrow = E.bits + ((int64_t)b * Wd + (i >> 5)) * L;
+  bool s_prev = false;
+  if (warp_valid && t0 - 1 >= tr.start && t0 >= 1)
+    s_prev = (bitrow[slot0 == 0 ? L - 1 : slot0 - 1] >> lane) & 1u;
+  st.keep = s_prev ? 0.f : 1.f;
+  st.m_fire = (fl & FIS_FL_FIRE_OFF) ? 0.f : 1.f;
+  st.m_in = (fl & FIS_FL_IN_OFF) ? 0.f : 1.f;
+  const bool hold = fl & FIS_FL_HOLD;
+  st.m_hold = hold ? 0.f : 1.f;
+  st.v_hold = hold ? tr.v_clamp : 0.f;
+  st.rs = (fl & FIS_FL_NOREFRAC) ? 0.f : E.p.refrac_steps;
+  const int64_t own0 = t0 - tr.start;  // the trial's own step at k = 0
 
-    // Poisson drive of the whole block (sim.py:859-861), before the step loop:
-    // draw j of neuron i is word j % 4 of Philox4x32-10 at counter
-    // (i, j / 4, trial lane); the (neuron, quad) pairs of the warp's driven
-    // neurons are spread over all 32 lanes, and each pair ORs its kick bits
-    // into the neuron's mask.
-    uint32_t dmask = 0;
-    if (!kTape) {
-      const float prob = __fmul_rn(rate, E.p.prob_scale);
-      const unsigned D = __ballot_sync(0xFFFFFFFFu, valid && ka < kb && prob > 0.f);
-      if (D) {
-        sdrive[threadIdx.x] = 0u;
-        sprob[threadIdx.x] = prob;
-        __syncwarp();
-        const int64_t own_a = own0 + ka;
-        const int64_t q0 = own_a >> 2;
-        const int nq = (int)(((own0 + kb - 1) >> 2) - q0) + 1;
-        const int total = __popc(D) * nq;
-        const int wbase = threadIdx.x - lane;
-        for (int it = lane; it < total; it += kWarp) {
-          const int jd = it / nq, qq = it - jd * nq;
-          unsigned m = D;
-          for (int t = 0; t < jd; ++t) m &= m - 1;
-          const int j = __ffs(m) - 1;
-          const int64_t quad = q0 + qq;
-          const Philox4 r4 = philox4((uint32_t)(i - lane + j), (uint32_t)quad,
-                                     (uint32_t)((uint64_t)quad >> 32), tr.stream,
-                                     (uint32_t)tr.seed, (uint32_t)(tr.seed >> 32));
-          const float pj = sprob[wbase + j];
-          uint32_t bits = 0;
+  // Poisson drive of the whole block (sim.py:859-861), before the step loop:
+  // draw j of neuron i is word j % 4 of Philox4x32-10 at counter
+  // (i, j / 4, trial lane); the (neuron, quad) pairs of the warp's driven
+  // neurons are spread over all 32 lanes, and each pair ORs its kick bits into
+  // the neuron's mask.
+  uint32_t dmask = 0;
+  bool warp_driven = false;
+  if (!kTape) {
+    const float prob = __fmul_rn(rate, E.p.prob_scale);
+    const unsigned D = __ballot_sync(0xFFFFFFFFu, valid && ka < kb && prob > 0.f);
+    warp_driven = D != 0u;
+    if (D) {
+      sdrive[threadIdx.x] = 0u;
+      sprob[threadIdx.x] = prob;
+      __syncwarp();
+      const int64_t q0 = (own0 + ka) >> 2;
+      const int nq = (int)(((own0 + kb - 1) >> 2) - q0) + 1;
+      const int total = __popc(D) * nq;
+      const int wbase = threadIdx.x - lane;
+      for (int it = lane; it < total; it += kWarp) {
+        const int jd = it / nq, qq = it - jd * nq;
+        unsigned m = D;
+        for (int t = 0; t < jd; ++t) m &= m - 1;
+        const int j = __ffs(m) - 1;
+        const int64_t quad = q0 + qq;
+        const Philox4 r4 = philox4((uint32_t)(i - lane + j), (uint32_t)quad,
+                                   (uint32_t)((uint64_t)quad >> 32), tr.stream,
+                                   (uint32_t)tr.seed, (uint32_t)(tr.seed >> 32));
+        const float pj = sprob[wbase + j];
+        uint32_t bits = 0;
 #pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            const int k = (int)(quad * 4 + q - own0);
-            if (k >= ka && k < kb && __fmul_rn((float)(r4.x[q] >> 8), 0x1p-24f) < pj)
-              bits |= 1u << k;
-          }
-          if (bits) atomicOr(&sdrive[wbase + j], bits);
+        for (int q = 0; q < 4; ++q) {
+          const int k = (int)(quad * 4 + q - own0);
+          if (k >= ka && k < kb && __fmul_rn((float)(r4.x[q] >> 8), 0x1p-24f) < pj)
+            bits |= 1u << k;
         }
-        __syncwarp();
-        dmask = sdrive[threadIdx.x];
+        if (bits) atomicOr(&sdrive[wbase + j], bits);
       }
+      __syncwarp();
+      dmask = sdrive[threadIdx.x];
     }
-    cp_async_wait_all();
+  }
 
-    const float kick = E.p.kick;
-    uint32_t fired_mask = 0;
-    // Both loops are entered by whole warps (ka, kb depend on the trial only),
-    // so every lane reaches each ballot; lanes past the last neuron (valid is
-    // false) hold zero input and skip the update.
-    if (ka == 0 && kb == K) {
-      // the whole block is inside the trial: the plain loop
-#pragma unroll 1
-      for (int k = 0; k < K; ++k) {
-        const int32_t c_in = sring[k][threadIdx.x];
-        // consumed slots return to zero: the scratch ring needs no clearing pass
-        if (c_in != 0) rp[k * sstride] = 0;
-        float sp = 0.f;
-        if (valid) {
-          const float vstim = kTape ? E.vstim[sidx] : (((dmask >> k) & 1u) ? kick : 0.f);
-          sp = lif_step(st, E.p, c_in, vstim);
-        }
-        const unsigned bal = __ballot_sync(0xFFFFFFFFu, sp != 0.f);
-        if (lane == 0) sbal[wib][k] = bal;
-        fired_mask |= (sp != 0.f ? 1u : 0u) << k;
+  // All staged copies are in shared memory: return the consumed ring slots to
+  // zero with one bulk copy per slot, so the scratch ring needs no clearing
+  // pass and the step loop no stores.
+  cp_async_wait_all();
+  fence_proxy_async_shared();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < K; ++k) bulk_store(rtile + (int64_t)k * sstride, szero, kTile * 4);
+    bulk_commit();
+  }
+
+  // Every lane of a warp runs the same loop (the choice depends on the trial
+  // and on the warp's ballot only), so every lane reaches each ballot.
+  float nspk;
+  if (kTape)
+    nspk = step_loop<true, false>(st, E, K, ka, kb, valid, 0u, sring, sbal[wib], lane, sidx);
+  else if (warp_driven)
+    nspk = step_loop<false, true>(st, E, K, ka, kb, valid, dmask, sring, sbal[wib], lane, sidx);
+  else
+    nspk = step_loop<false, false>(st, E, K, ka, kb, valid, 0u, sring, sbal[wib], lane, sidx);
+  __syncwarp();
+  // the raster words of the K steps into the ring of the last L steps
+  if (lane < K && warp_valid) {
+    const int sl = slot0 + lane < L ? slot0 + lane : slot0 + lane - L;
+    bitrow[sl] = sbal[wib][lane];
+  }
+
+  if (valid && ka < kb) {
+    E.v[sidx] = st.v;
+    E.g[sidx] = st.g;
+    E.refrac[sidx] = st.r;
+  }
+  if (spikes_out && valid) spikes_out[sidx] = (st.keep == 0.f) ? 1.f : 0.f;
+
+  // Spike lists and recording for the (rare) steps this neuron fired; the
+  // steps are read back from the staged raster words.
+  if (nspk != 0.f) {
+    const int B = E.batch;
+    const bool out_on = !(fl & (FIS_FL_OUT_OFF | FIS_FL_SILENCED));
+    const int nch = E.nchunks[i];
+    const int slot20 = (int)mod_pos(t0, 2 * L);
+    for (int k = 0; k < K; ++k) {
+      if (!((sbal[wib][k] >> lane) & 1u)) continue;
+      const int sl = slot0 + k < L ? slot0 + k : slot0 + k - L;
+      const int sl2 = slot20 + k < 2 * L ? slot20 + k : slot20 + k - 2 * L;
+      if ((out_on || k == K - 1) && nch > 0) {
+        const int32_t pos = atomicAdd(E.list_len + (int64_t)sl2 * B + b, nch);
+        uint32_t* dst = E.lists + ((int64_t)sl * B + b) * E.list_cap;
+        for (int q = 0; q < nch; ++q)
+          if (pos + q < E.list_cap) dst[pos + q] = ((uint32_t)i << 8) | (uint32_t)q;
       }
-    } else {
-#pragma unroll 1
-      for (int k = 0; k < K; ++k) {
-        const int32_t c_in = sring[k][threadIdx.x];
-        if (valid && c_in != 0) rp[k * sstride] = 0;
-        float sp = 0.f;
-        if (valid && k >= ka && k < kb) {
-          const float vstim = kTape ? E.vstim[sidx] : (((dmask >> k) & 1u) ? kick : 0.f);
-          sp = lif_step(st, E.p, c_in, vstim);
-        }
-        const unsigned bal = __ballot_sync(0xFFFFFFFFu, sp != 0.f);
-        if (lane == 0) sbal[wib][k] = bal;
-        fired_mask |= (sp != 0.f ? 1u : 0u) << k;
-      }
-    }
-    __syncwarp();
-    // the raster words of the K steps into the ring of the last L steps
-    if (lane < K) {
-      const int sl = slot0 + lane < L ? slot0 + lane : slot0 + lane - L;
-      bitrow[sl] = sbal[wib][lane];
-    }
-
-    if (valid && ka < kb) {
-      E.v[sidx] = st.v;
-      E.g[sidx] = st.g;
-      E.refrac[sidx] = st.r;
-    }
-    if (spikes_out && valid) spikes_out[sidx] = (st.keep == 0.f) ? 1.f : 0.f;
-
-    // Spike lists and recording for the (rare) steps this neuron fired.
-    if (fired_mask) {
-      const int B = E.batch;
-      const bool out_on = !(fl & (FIS_FL_OUT_OFF | FIS_FL_SILENCED));
-      const int nch = E.nchunks[i];
-      const int slot20 = (int)mod_pos(t0, 2 * L);
-      while (fired_mask) {
-        const int k = __ffs(fired_mask) - 1;
-        fired_mask &= fired_mask - 1;
-        const int sl = slot0 + k < L ? slot0 + k : slot0 + k - L;
-        const int sl2 = slot20 + k < 2 * L ? slot20 + k : slot20 + k - 2 * L;
-        if ((out_on || k == K - 1) && nch > 0) {
-          const int32_t pos = atomicAdd(E.list_len + (int64_t)sl2 * B + b, nch);
-          uint32_t* dst = E.lists + ((int64_t)sl * B + b) * E.list_cap;
-          for (int q = 0; q < nch; ++q)
-            if (pos + q < E.list_cap) dst[pos + q] = ((uint32_t)i << 8) | (uint32_t)q;
-        }
-        if (tr.rec >= 0 && tr.rec < E.n_recs && tr.bin_steps > 0) {
-          const int64_t bin = (own0 + k) / tr.bin_steps;
-          if (bin < tr.n_bins) atomicAdd(E.recs[tr.rec] + bin * n + i, 1);
-        }
+      if (tr.rec >= 0 && tr.rec < E.n_recs && tr.bin_steps > 0) {
+        const int64_t bin = (own0 + k) / tr.bin_steps;
+        if (bin < tr.n_bins) atomicAdd(E.recs[tr.rec] + bin * n + i, 1);
       }
     }
   }
+
+  // The clearing copies complete before the CTA ends (szero must stay valid
+  // while they read it, and the next scatter adds into these lines).
+  if (threadIdx.x == 0) bulk_wait_all();
 
   if (bump) {
     __syncthreads();
@@ -496,13 +560,17 @@ __global__ void k_load_spikes(const fis_engine E, int b0, int nb,
   }
 }
 
-__global__ void k_add_rows(int64_t row_elems, int rows, const int32_t* __restrict__ src,
-                           int64_t ss, int32_t* __restrict__ dst, int64_t ds) {
-  const int64_t total = row_elems * rows;
+// dst[r][b][i] += src[r][b][i] with separate row and trial strides.
+__global__ void k_add_rows(int n, int nb, int rows, const int32_t* __restrict__ src, int64_t ss,
+                           int64_t st, int32_t* __restrict__ dst, int64_t ds, int64_t dt) {
+  const int64_t total = (int64_t)rows * nb * n;
   for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < total;
        x += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t r = x / row_elems, e = x - r * row_elems;
-    dst[r * ds + e] += src[r * ss + e];
+    const int i = (int)(x % n);
+    const int64_t rb = x / n;
+    const int bb = (int)(rb % nb);
+    const int64_t r = rb / nb;
+    dst[r * ds + bb * dt + i] += src[r * ss + bb * st + i];
   }
 }
 
@@ -561,9 +629,9 @@ static int check_block(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_st
   if (k_steps < 1 || k_steps > FIS_MAX_BLOCK || k_steps > e->p.lag) return FIS_E_BOUNDS;
   if (e->vstim && k_steps != 1) return FIS_E_BOUNDS;
   if ((k_steps + 1) * nb + 1 > kMaxLists) return FIS_E_BOUNDS;
-  const int64_t threads = (int64_t)nb * ((e->n + kWarp - 1) / kWarp) * kWarp;
-  if (threads + kUpdThreads > 0x7FFFFFFFLL) return FIS_E_BOUNDS;
-  if ((int64_t)nb * e->n * FIS_MAX_BLOCK > 0x7FFFFFFFLL) return FIS_E_BOUNDS;
+  const int64_t rows = (int64_t)nb * ring_row(e->n);
+  if (rows * FIS_MAX_BLOCK > 0x7FFFFFFFLL) return FIS_E_BOUNDS;
+  if (((uintptr_t)ring & 15u) != 0) return FIS_E_ALIGN;
   return FIS_OK;
 }
 
@@ -580,6 +648,7 @@ int fis_scatter(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, in
   A.zero_next = k_steps;
   A.filter_last = 1;
   A.ring = ring;
+  A.trial_stride = ring_row(e->n);
   const size_t smem = sizeof(int32_t) * (size_t)((k_steps + 1) * nb + 1);
   k_scatter<<<sm_count() * 4, kScatThreads, smem, (cudaStream_t)stream>>>(*e, A);
   return launch_status();
@@ -589,8 +658,7 @@ int fis_update(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, int
                float* spikes_out, int32_t last_group, void* stream) {
   const int rc = check_block(e, b0, nb, k_steps, ring);
   if (rc) return rc;
-  const int64_t threads = (int64_t)nb * ((e->n + kWarp - 1) / kWarp) * kWarp;
-  const int64_t ugrid = (threads + kUpdThreads - 1) / kUpdThreads;
+  const int64_t ugrid = (int64_t)nb * (ring_row(e->n) / kTile);
   if (e->vstim)
     k_update<true><<<(unsigned)ugrid, kUpdThreads, 0, (cudaStream_t)stream>>>(
         *e, b0, nb, k_steps, ring, spikes_out, last_group ? 1 : 0);
@@ -660,6 +728,7 @@ int fis_delay_buffer(const fis_engine* e, int32_t b0, int32_t nb, int32_t* scrat
   A.zero_next = 0;
   A.filter_last = 0;
   A.ring = scratch;
+  A.trial_stride = e->n;
   const size_t smem = sizeof(int32_t) * (size_t)((R + 1) * nb + 1);
   k_scatter<<<sm_count() * 4, kScatThreads, smem, st>>>(*e, A);
   if ((rc = launch_status())) return rc;
@@ -693,15 +762,21 @@ int fis_load_spikes(const fis_engine* e, int32_t b0, int32_t nb, const float* sp
 }
 
 int fis_add_rows(const fis_engine* e, int32_t nb, int32_t rows, const int32_t* src,
-                 int64_t src_row_stride, int32_t* dst, int64_t dst_row_stride,
-                 void* stream) {
+                 int64_t src_row_stride, int64_t src_trial_stride, int32_t* dst,
+                 int64_t dst_row_stride, int64_t dst_trial_stride, void* stream) {
   if (!e || !src || !dst || nb < 1 || rows < 0) return FIS_E_ARG;
   if (rows == 0) return FIS_OK;
-  const int64_t row_elems = (int64_t)nb * e->n;
-  if (src_row_stride < row_elems || dst_row_stride < row_elems) return FIS_E_BOUNDS;
-  k_add_rows<<<grid_for(row_elems * rows, 256), 256, 0, (cudaStream_t)stream>>>(
-      row_elems, rows, src, src_row_stride, dst, dst_row_stride);
+  if (src_trial_stride < e->n || dst_trial_stride < e->n ||
+      src_row_stride < (int64_t)(nb - 1) * src_trial_stride + e->n ||
+      dst_row_stride < (int64_t)(nb - 1) * dst_trial_stride + e->n)
+    return FIS_E_BOUNDS;
+  const int64_t total = (int64_t)rows * nb * e->n;
+  k_add_rows<<<grid_for(total, 256), 256, 0, (cudaStream_t)stream>>>(
+      e->n, nb, rows, src, src_row_stride, src_trial_stride, dst, dst_row_stride,
+      dst_trial_stride);
   return launch_status();
 }
+
+int fis_ring_row(int32_t n) { return n < 1 ? FIS_E_ARG : ring_row(n); }
 
 }  // extern "C"

@@ -36,7 +36,8 @@ STATUS = {0: "ok", -1: "FIS_E_ARG (null pointer or size out of range)",
 EXPORTS = ("ev_spmv_i32", "ev_spmv_i64", "ev_spmv_abi", "fis_abi",
            "fis_sizeof_engine", "fis_sizeof_trial", "fis_check", "fis_block",
            "fis_scatter", "fis_update", "fis_advance",
-           "fis_delay_buffer", "fis_spikes_f32", "fis_load_spikes", "fis_add_rows")
+           "fis_delay_buffer", "fis_spikes_f32", "fis_load_spikes", "fis_add_rows",
+           "fis_ring_row")
 
 
 class KernelUnavailable(RuntimeError):
@@ -106,7 +107,9 @@ def load(path=None):
     L.fis_delay_buffer.argtypes = [P, I32, I32, P, P, P]
     L.fis_spikes_f32.argtypes = [P, I32, I32, I64, P, P]
     L.fis_load_spikes.argtypes = [P, I32, I32, P, P]
-    L.fis_add_rows.argtypes = [P, I32, I32, P, I64, P, I64, P]
+    L.fis_add_rows.argtypes = [P, I32, I32, P, I64, I64, P, I64, I64, P]
+    L.fis_ring_row.argtypes = [I32]
+    L.fis_ring_row.restype = ctypes.c_int
     L.ev_spmv_i32.argtypes = [P, P, P, P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P]
     L.ev_spmv_i64.argtypes = [P, P, P, P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P]
     for s in ("fis_check", "fis_block", "fis_scatter", "fis_update", "fis_advance",

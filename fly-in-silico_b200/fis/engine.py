@@ -178,9 +178,10 @@ class Core:
         if group is None:
             group = max(1, RING_L2_BYTES // (self.max_block * self.n * 4))
         self.group = int(max(1, min(int(group), self.batch)))
+        self.ring_row = int(self.lib.fis_ring_row(self.n))
         with torch.cuda.device(self.device):
-            self.ring = torch.zeros((self.max_block, self.group, self.n), dtype=torch.int32,
-                                    device=self.device)
+            self.ring = torch.zeros((self.max_block, self.group, self.ring_row),
+                                    dtype=torch.int32, device=self.device)
 
     def set_recordings(self, bufs):
         """Recording buffers, each int32 [n_bins][N]; trials point at them by index."""
@@ -260,13 +261,13 @@ class Core:
         lo, hi = max(t0, p0), min(t0 + k, p0 + self.buf_len)
         if lo >= hi:
             return
-        n = self.n
+        n, NR = self.n, self.ring_row
         src = rows[lo - p0, g0]  # [nb][N] starts here; row stride B*N
-        # the kernel's ring for this group is [k][nb][N]: row stride nb*N
+        # the kernel's ring for this group is [k][nb][NR]
         rc = self.lib.fis_add_rows(ctypes.byref(self.desc), nb, hi - lo,
-                                   ctypes.c_void_p(src.data_ptr()), self.batch * n,
-                                   ctypes.c_void_p(self.ring.data_ptr() + (lo - t0) * nb * n * 4),
-                                   nb * n, ctypes.c_void_p(st))
+                                   ctypes.c_void_p(src.data_ptr()), self.batch * n, n,
+                                   ctypes.c_void_p(self.ring.data_ptr() + (lo - t0) * nb * NR * 4),
+                                   nb * NR, NR, ctypes.c_void_p(st))
         _lib.check(rc, "fis_add_rows")
 
     def advance(self, steps, spikes_out=None, timer=None, events=None, every=1):

@@ -170,7 +170,9 @@ int fis_check(const fis_engine* e);
  * k_steps steps (refractory gate, delayed input, conductance, Poisson drive,
  * membrane, hold, threshold, reset).  Replaces one call of Engine.step per
  * step (sim.py:745-771, 863-953).
- *   ring        int32 [k_steps][nb][N], all zero on entry, all zero on exit
+ *   ring        int32 [k_steps][nb][NR], NR = fis_ring_row(N) (N rounded up
+ *               to a multiple of 256), 16-byte aligned; all zero on entry,
+ *               all zero on exit
  *   spikes_out  float [B][N] or NULL: the spikes of the block's last step
  *   last_group  nonzero when this call completes the block for all trial
  *               groups; the device clock then advances by k_steps
@@ -192,7 +194,7 @@ int fis_update(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps,
  * steps (the last one shorter), each block running fis_scatter + fis_update
  * for the trial groups [g0, g0+group) in turn.  The native form of a host
  * loop over fis_block.
- *   ring        int32 [min(FIS_MAX_BLOCK, lag)][group][N], zero on entry
+ *   ring        int32 [min(FIS_MAX_BLOCK, lag)][group][NR], zero on entry
  *   spikes_out  float [B][N] or NULL, written by the last block
  *   events      NULL, or 2*n_pairs cudaEvent_t handles: pair j is recorded
  *               around the update launch number j*every (0-based over the
@@ -226,12 +228,16 @@ int fis_spikes_f32(const fis_engine* e, int32_t b0, int32_t nb, int64_t step,
 int fis_load_spikes(const fis_engine* e, int32_t b0, int32_t nb,
                     const float* spikes, void* stream);
 
-/* dst[r][b][i] += src[r][b][i] for r < rows, b < nb, i < N, with the row
- * strides given in elements (restore path: pending delayed input that a
+/* dst[r][b][i] += src[r][b][i] for r < rows, b < nb, i < N, with row and
+ * trial strides given in elements (restore path: pending delayed input that a
  * restored delay ring holds for the next buf_len steps). */
 int fis_add_rows(const fis_engine* e, int32_t nb, int32_t rows,
-                 const int32_t* src, int64_t src_row_stride, int32_t* dst,
-                 int64_t dst_row_stride, void* stream);
+                 const int32_t* src, int64_t src_row_stride,
+                 int64_t src_trial_stride, int32_t* dst, int64_t dst_row_stride,
+                 int64_t dst_trial_stride, void* stream);
+
+/* Row length NR of the scratch ring for N neurons (N rounded up to 256). */
+int fis_ring_row(int32_t n);
 
 #ifdef __cplusplus
 }
