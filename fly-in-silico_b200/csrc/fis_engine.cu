@@ -31,6 +31,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "fis_common.cuh"
 
@@ -780,3 +781,68 @@ int fis_add_rows(const fis_engine* e, int32_t nb, int32_t rows, const int32_t* s
 int fis_ring_row(int32_t n) { return n < 1 ? FIS_E_ARG : ring_row(n); }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// fis_block_noalloc: the block step with the scratch ring inside the library
+// ---------------------------------------------------------------------------
+//
+// Some callers cannot allocate device memory for the scratch ring that
+// fis_block takes: a closed-loop controller that steps the brain inside a hard
+// real-time budget per control step (a device allocation can synchronize the
+// whole GPU and stall for milliseconds), or a host that binds only this C ABI
+// from another language and has no device allocator of its own to hand out a
+// buffer.  For them the ring is a fixed array in this library:
+//
+//  * it holds FIS_NOALLOC_RING_INTS int32 (12 MiB): one trial of the
+//    138,639-neuron connectome in 20-step blocks; a call that needs more
+//    (k_steps * nb * fis_ring_row(n) elements) is refused with FIS_E_BOUNDS;
+//  * every GPU that loads this library holds the array until the process
+//    exits;
+//  * all calls on one device share it, so calls that overlap on the GPU (from
+//    other streams or threads) race on it and must not be issued concurrently;
+//  * each call clears the part it uses before its scatter, so it never
+//    depends on what an earlier, possibly failed, call left there;
+//  * the first call on each device looks up the array's device address with
+//    that device current; make that first call before any stream capture.
+
+namespace {
+
+__device__ __align__(256) int32_t g_noalloc_ring[FIS_NOALLOC_RING_INTS];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+int32_t* g_noalloc_addr[kMaxDevices] = {};
+
+// Device address of g_noalloc_ring on the current device, looked up once per
+// device (host code cannot use the symbol itself as a device pointer).
+int noalloc_ring(int32_t** out) {
+  int dev = -1;
+  cudaError_t err = cudaGetDevice(&dev);
+  if (err != cudaSuccess) return (int)err;
+  if (dev < 0 || dev >= kMaxDevices) return FIS_E_ARG;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    err = cudaGetSymbolAddress(&p, g_noalloc_ring);
+    if (err != cudaSuccess) return (int)err;
+    g_noalloc_addr[dev] = static_cast<int32_t*>(p);
+  }
+  *out = g_noalloc_addr[dev];
+  return FIS_OK;
+}
+
+}  // namespace
+
+extern "C" int fis_block_noalloc(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps,
+                                 float* spikes_out, int32_t last_group, void* stream) {
+  int rc = fis_check(e);
+  if (rc) return rc;
+  if (nb < 1 || k_steps < 1) return FIS_E_BOUNDS;
+  const int64_t need = (int64_t)k_steps * nb * ring_row(e->n);
+  if (need > (int64_t)FIS_NOALLOC_RING_INTS) return FIS_E_BOUNDS;
+  int32_t* ring = nullptr;
+  if ((rc = noalloc_ring(&ring))) return rc;
+  rc = (int)cudaMemsetAsync(ring, 0, sizeof(int32_t) * (size_t)need, (cudaStream_t)stream);
+  if (rc) return rc;
+  return fis_block(e, b0, nb, k_steps, ring, spikes_out, last_group, stream);
+}

@@ -19,6 +19,7 @@ LIB_PATH = PKG / LIB_NAME
 
 FIS_ABI_VERSION = 1
 FIS_MAX_BLOCK = 20
+FIS_NOALLOC_RING_INTS = 3 << 20
 REF_EV_ABI = 3
 
 FIS_FL_FIRE_OFF = 1 << 0
@@ -37,7 +38,7 @@ EXPORTS = ("ev_spmv_i32", "ev_spmv_i64", "ev_spmv_abi", "fis_abi",
            "fis_sizeof_engine", "fis_sizeof_trial", "fis_check", "fis_block",
            "fis_scatter", "fis_update", "fis_advance",
            "fis_delay_buffer", "fis_spikes_f32", "fis_load_spikes", "fis_add_rows",
-           "fis_ring_row")
+           "fis_ring_row", "fis_block_noalloc")
 
 
 class KernelUnavailable(RuntimeError):
@@ -108,6 +109,8 @@ def load(path=None):
     L.fis_spikes_f32.argtypes = [P, I32, I32, I64, P, P]
     L.fis_load_spikes.argtypes = [P, I32, I32, P, P]
     L.fis_add_rows.argtypes = [P, I32, I32, P, I64, I64, P, I64, I64, P]
+    L.fis_block_noalloc.argtypes = [P, I32, I32, I32, P, I32, P]
+    L.fis_block_noalloc.restype = ctypes.c_int
     L.fis_ring_row.argtypes = [I32]
     L.fis_ring_row.restype = ctypes.c_int
     L.ev_spmv_i32.argtypes = [P, P, P, P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P]

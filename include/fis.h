@@ -239,6 +239,22 @@ int fis_add_rows(const fis_engine* e, int32_t nb, int32_t rows,
 /* Row length NR of the scratch ring for N neurons (N rounded up to 256). */
 int fis_ring_row(int32_t n);
 
+/*
+ * fis_block without the `ring` argument: the scratch ring is a fixed array
+ * of FIS_NOALLOC_RING_INTS int32 (12 MiB) inside this library, for callers
+ * that cannot allocate device memory (a real-time closed-loop controller,
+ * where an allocation may stall the GPU; a foreign-language host with no
+ * device allocator).  No counterpart in the reference.  Larger blocks
+ * (k_steps * nb * fis_ring_row(N) > FIS_NOALLOC_RING_INTS) return
+ * FIS_E_BOUNDS.  Every GPU that loads the library keeps the array until
+ * exit; calls overlapping on the GPU race on it; each call clears what it
+ * uses; the first call on a device looks up the array's address and should
+ * come before any stream capture.
+ */
+#define FIS_NOALLOC_RING_INTS (3 << 20)
+int fis_block_noalloc(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps,
+                      float* spikes_out, int32_t last_group, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

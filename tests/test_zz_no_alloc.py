@@ -1,0 +1,82 @@
+"""The allocation-free block step, checked against the regular one.
+
+``fis_block`` takes a scratch ring from its caller.  Some callers cannot
+allocate one: a closed-loop controller that steps the brain inside a hard
+real-time budget (a device allocation may synchronize the GPU and stall for
+milliseconds), or a host binding only the C ABI with no device allocator of
+its own.  ``fis_block_noalloc`` keeps the ring in a fixed 12 MiB array inside
+the library.  This file is collected last on purpose: it runs after every
+other GPU test, and also passes alone in a fresh process.
+"""
+
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _engine(conn, drive):
+    import fis._lib as L
+    from fis.engine import Core
+
+    core = Core(conn, 1, group=1)
+    idx = torch.as_tensor(drive, device=core.device)
+    core.rates[0, idx] = 150.0
+    core.flags[0, idx] |= L.FIS_FL_NOREFRAC
+    core.reset_slots(slice(None))
+    core.trials[0].seed = 11
+    core.mark_trials()
+    return core
+
+
+def test_noalloc_block_matches_block_on_two_calls():
+    import fis._lib as L
+    import fis.connectome as C
+
+    conn = C.synthetic()  # the full 138,639-neuron connectome
+    drive = np.sort(np.random.default_rng(7).choice(conn.n, 2249, replace=False))
+    a, b = _engine(conn, drive), _engine(conn, drive)
+    a.advance(200)  # spikes in flight through the delay
+    b.advance(200)
+    lib = L.load()
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    sa = torch.zeros((1, conn.n), device=a.device)
+    sb = torch.zeros((1, conn.n), device=b.device)
+    for call in range(2):
+        a._sync_trials()
+        b._sync_trials()
+        rc = lib.fis_block(ctypes.byref(a.desc), 0, 1, 20, ctypes.c_void_p(a.ring.data_ptr()),
+                           ctypes.c_void_p(sa.data_ptr()), 1, stream)
+        assert rc == 0
+        rc = lib.fis_block_noalloc(ctypes.byref(b.desc), 0, 1, 20,
+                                   ctypes.c_void_p(sb.data_ptr()), 1, stream)
+        assert rc == 0
+        a.step += 20
+        b.step += 20
+        torch.cuda.synchronize()
+        for x, y in ((a.v, b.v), (a.g, b.g), (a.refrac, b.refrac), (sa, sb),
+                     (a.bits, b.bits), (a.list_len, b.list_len), (a.clock, b.clock)):
+            assert torch.equal(x, y), call
+        assert int(sa.sum()) > 0 or call == 0 or int(a.bits.ne(0).sum()) > 0
+
+
+def test_noalloc_refuses_blocks_larger_than_its_array():
+    import fis._lib as L
+    import fis.connectome as C
+
+    conn = C.synthetic()
+    drive = np.arange(100)
+    core = _engine(conn, drive)
+    lib = L.load()
+    nr = lib.fis_ring_row(conn.n)
+    assert 20 * 1 * nr <= L.FIS_NOALLOC_RING_INTS < 20 * 2 * nr
+    from fis.engine import Core
+
+    two = Core(conn, 2, group=2)
+    rc = lib.fis_block_noalloc(ctypes.byref(two.desc), 0, 2, 20, None, 1,
+                               ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    assert rc == -2  # FIS_E_BOUNDS, nothing launched
+    del core
