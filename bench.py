@@ -39,9 +39,13 @@ WORKLOAD = ("batched 64 trials x 10,000 steps (1 s), N=138,639, E=15,091,983 syn
             "1-100 silenced")
 SPEC_SEED = 2024
 CONN_SEED = 0
-# Update-kernel DRAM traffic per launch from the committed ncu capture
-# (profiles/k_update_ncu.md); None until measured.
-NCU_TRAFFIC_PER_LAUNCH = None
+# Update-kernel DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum)
+# per trial-neuron and block, from the ncu capture summarised in
+# profiles/k_update_batched64.md (74.7 MB for one launch of 8 trials x 138,639
+# neurons x 20 steps; ncu flushes caches between replay passes, so this counts
+# the scratch ring as cold reads and is an upper bound).  Scaled to the
+# bench's launch size by the neurons it processes.
+NCU_TRAFFIC_PER_NEURON_BLOCK = 74.75e6 / (8 * 138_639)
 
 
 def parse():
@@ -54,7 +58,59 @@ def parse():
     ap.add_argument("--sim-steps", type=int, default=SIM_STEPS)
     ap.add_argument("--group", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--quick", action="store_true",
+                    help="skip the uneven-duration and serving measurements")
     return ap.parse_args()
+
+
+def uneven_run(conn, group):
+    """256 trials, durations U[500, 20,000] steps, retired in place as they end."""
+    import torch
+
+    from fis.batch import Batch, random_specs
+
+    specs = random_specs(conn.n, 256, SPEC_SEED + 7, (500, 20000))
+    b = Batch(conn, 256, group=group)
+    b.run(specs[:8])  # warm the allocations
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    b.run(specs)
+    e.record()
+    torch.cuda.synchronize()
+    ms = s.elapsed_time(e)
+    trial_steps = sum(int(x.steps) for x in specs)
+    del b
+    torch.cuda.empty_cache()
+    return {"value": trial_steps * conn.n / (ms / 1000.0), "unit": "neuron-steps/s",
+            "trials": 256, "durations": "U[500, 20000] steps", "trial_steps": trial_steps,
+            "ms": ms, "how": "host trial specs in, host counts out; finished trials frozen "
+                             "in place until the longest ends"}
+
+
+def serving_run(conn, group, plain_value):
+    """Open-loop stream: Poisson arrivals at 2 req/s, 1-64 trials, 1,000-50,000 steps."""
+    import torch
+
+    from fis.serve import Server, poisson_requests
+
+    reqs = poisson_requests(conn.n, SPEC_SEED + 9, 2.0, 12, trials=(1, 64),
+                            steps=(1000, 50000), bin_steps=100)
+    srv = Server(conn, capacity=256, group=group)
+    t0 = time.perf_counter()
+    replies = srv.run(reqs, realtime=True)
+    wall = time.perf_counter() - t0
+    lat = Server.latency_stats(replies)
+    units = sum(r.trial_steps for r in replies) * conn.n
+    out = {"requests": len(replies), "arrival_rate_hz": 2.0, "p50_s": lat["p50_s"],
+           "p99_s": lat["p99_s"], "mean_s": lat["mean_s"],
+           "throughput": units / wall, "unit": "neuron-steps/s", "wall_s": wall,
+           "serial_plain_s": units / plain_value if plain_value else None,
+           "how": "Poisson arrivals, admission by free slots and recording memory, "
+                  "continuous batching into 256 slots, 10 ms bins per request"}
+    del srv
+    torch.cuda.empty_cache()
+    return out
 
 
 def dist_env():
@@ -206,9 +262,15 @@ def main():
     import fis.connectome as C
     from fis.batch import Batch, random_specs
 
+    from fis.tune import tune
+
     conn = C.synthetic(seed=CONN_SEED)
     specs = random_specs(conn.n, args.trials, SPEC_SEED + 1000 * rank, args.sim_steps)
-    batch = Batch(conn, args.trials, group=args.group)
+    if args.group is None:
+        best = tune(conn, args.trials)
+    else:
+        best = {"group": args.group, "chunk": None, "candidates": []}
+    batch = Batch(conn, args.trials, group=best["group"], chunk=best["chunk"])
     core = batch.core
     slots = list(range(args.trials))
     batch.load(slots, specs)
@@ -220,7 +282,7 @@ def main():
             t.end = core.step + specs[b].steps
         core.mark_trials()
         core.reset_slots(slice(None))
-        for r in batch._recs:
+        for r in batch.recordings():
             r.zero_()
         core.advance(args.sim_steps, events=events, every=every)
 
@@ -323,9 +385,15 @@ def main():
         alg = bytes_launch
         achieved = bytes_launch / (upd_ms / 1000.0) / 1e9
         roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "traffic": NCU_TRAFFIC_PER_LAUNCH,
+                "frac": achieved / hbm,
+                "traffic": NCU_TRAFFIC_PER_NEURON_BLOCK * G * conn.n,
                 "kernel": "k_update", "launch_ms": upd_ms,
                 "algorithmic_bytes_per_launch": alg, "peak_kind": peak_kind}
+
+    uneven = serving = None
+    if rank == 0 and not args.quick:
+        uneven = uneven_run(conn, core.group)
+        serving = serving_run(conn, core.group, plain["value"] if plain else None)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -344,7 +412,8 @@ def main():
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "trials_per_gpu": args.trials,
-                       "sim_steps": args.sim_steps, "trial_group": core.group,
+                       "sim_steps": args.sim_steps, "trial_group": core.group, "scatter_chunk": core.chunk,
+                       "autotune_candidates": len(best["candidates"]),
                        "block_steps": core.max_block,
                        "l2": "inputs larger than L2 (trial state 150 MB, spike lists "
                              "%.0f MB, CSR 60 MB)" % (core.lists.numel() * 4 / 1e6),
@@ -356,6 +425,8 @@ def main():
             "roofline": roof,
             "plain_1trial": plain,
             "batched_over_plain": (value / world) / plain["value"] if plain else None,
+            "uneven_256": uneven,
+            "serving": serving,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line))

@@ -73,6 +73,12 @@ __device__ __forceinline__ void fence_proxy_async_shared() {
   asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
 }
 
+// x mod m for 0 <= x < 4m (slot arithmetic on small offsets).
+__device__ __forceinline__ int wrap(int x, int m) {
+  while (x >= m) x -= m;
+  return x;
+}
+
 // Ring rows are padded per trial to a whole number of update tiles.
 constexpr int kTile = 256;
 __host__ __device__ __forceinline__ int ring_row(int n) { return (n + kTile - 1) / kTile * kTile; }
@@ -109,9 +115,13 @@ struct ScatterArgs {
   int slot_mode;      // 0: slot kk; 1: the reference ring slot (u + 1) % buf_len
   int zero_next;      // zero list_len of steps clock .. clock+zero_next-1
   int filter_last;    // handle the list of step clock-1 as described above
-  int32_t* ring;      // slot stride nb*trial_stride
+  int32_t* ring;      // slot stride nb*trial_stride elements
   int trial_stride;   // elements per trial row of `ring`
+  int half;           // elements are biased uint16 (see fis.h), else int32
 };
+
+// The value that marks an empty pair of biased uint16 ring elements.
+constexpr uint32_t kEmptyPair = 0x80008000u;
 
 __global__ void __launch_bounds__(kScatThreads)
 k_scatter(const fis_engine E, const ScatterArgs A) {
@@ -119,9 +129,14 @@ k_scatter(const fis_engine E, const ScatterArgs A) {
   const int n = E.n;
   const int B = E.batch;
   const int L = E.p.lag;
-  const int64_t t0 = *E.clock;
-  const int64_t u_first = t0 + A.u_off;
+  const fis_clock ck = *E.clock;
+  const int64_t t0 = ck.step;
+  const int64_t u_first = t0 + A.u_off;  // u_off is -lag: u_first = t0 mod lag
   const int64_t u_last = t0 - 1;
+  // slots of step u_first + kk: (ck.slot + kk) mod L and (ck.slot2 + L + kk) mod 2L
+  const int slot_last = wrap(ck.slot + L - 1, L);
+  const int slot2_last = wrap(ck.slot2 + 2 * L - 1, 2 * L);
+  const int t_mod_r = A.slot_mode ? (int)mod_pos(t0, E.p.buf_len) : 0;
   // Is the list of step t0-1 one of the sources?
   const int kk_last = (int)(u_last - u_first);
   const bool last_is_src = A.filter_last && kk_last >= 0 && kk_last < A.nsrc;
@@ -136,8 +151,9 @@ k_scatter(const fis_engine E, const ScatterArgs A) {
     for (int j = j0; j < j0 + per && j < nlists; ++j) {
       const int kk = j / A.nb, bl = j - kk * A.nb;
       const int64_t u = (kk < A.nsrc) ? u_first + kk : u_last;
+      const int s2 = (kk < A.nsrc) ? wrap(ck.slot2 + L + kk, 2 * L) : slot2_last;
       int32_t len = 0;
-      if (u >= 0) len = E.list_len[mod_pos(u, 2 * L) * B + A.b0 + bl];
+      if (u >= 0) len = E.list_len[s2 * B + A.b0 + bl];
       pre_sum[j] = len;  // provisional
       acc += len;
     }
@@ -167,7 +183,7 @@ k_scatter(const fis_engine E, const ScatterArgs A) {
   if (blockIdx.x == 0) {
     for (int j = threadIdx.x; j < A.zero_next * A.nb; j += blockDim.x) {
       const int kk = j / A.nb, bl = j - kk * A.nb;
-      E.list_len[mod_pos(t0 + kk, 2 * L) * B + A.b0 + bl] = 0;
+      E.list_len[wrap(ck.slot2 + kk, 2 * L) * B + A.b0 + bl] = 0;
     }
   }
 
@@ -186,7 +202,8 @@ k_scatter(const fis_engine E, const ScatterArgs A) {
     const int b = A.b0 + bl;
     const bool is_src = kk < A.nsrc;
     const int64_t u = is_src ? u_first + kk : u_last;
-    uint32_t* lst = E.lists + ((int64_t)mod_pos(u, L) * B + b) * E.list_cap;
+    const int su = is_src ? wrap(ck.slot + kk, L) : slot_last;
+    uint32_t* lst = E.lists + ((int64_t)su * B + b) * E.list_cap;
     const int32_t idx = w - pre_sum[j];
     if (idx >= E.list_cap) continue;
     const uint32_t e = lst[idx];
@@ -204,8 +221,11 @@ k_scatter(const fis_engine E, const ScatterArgs A) {
     const int64_t lo_e = r0 + (int64_t)entry_chunk(e) * E.chunk;
     const int64_t hi_e = min(r1, lo_e + (int64_t)E.chunk);
     if (lo_e >= hi_e) continue;
-    const int slot = A.slot_mode ? (int)mod_pos(u + 1, E.p.buf_len) : kk;
-    int32_t* dst = A.ring + slot * slot_stride + (int64_t)bl * A.trial_stride;
+    // slot_mode 1: (u + 1) mod buf_len = (t0 + kk) mod buf_len, as lag = buf_len + 1
+    const int slot = A.slot_mode ? wrap(t_mod_r + kk, E.p.buf_len) : kk;
+    const int64_t row = slot * slot_stride + (int64_t)bl * A.trial_stride;
+    int32_t* dst = A.ring + row;
+    uint16_t* dst16 = reinterpret_cast<uint16_t*>(A.ring) + row;
     // 16-byte vector loads: four edges per lane, 128 edges per warp pass.
     for (int64_t p = (lo_e & ~(int64_t)3) + 4 * lane; p < hi_e; p += 4 * kWarp) {
       const uint4 q = __ldg(reinterpret_cast<const uint4*>(E.edges + p));
@@ -215,7 +235,16 @@ k_scatter(const fis_engine E, const ScatterArgs A) {
         const int64_t pe = p + c;
         if (pe >= lo_e && pe < hi_e) {
           const int post = edge_post(wv[c]);
-          if (post < n) atomicAdd(dst + post, edge_count(wv[c]));
+          if (post < n) {
+            if (A.half) {
+              // the pair (post & ~1, post | 1) shares one 32-bit word (rows
+              // are even-sized, so pairs never straddle a row)
+              uint32_t* w = reinterpret_cast<uint32_t*>(dst16 + (post & ~1));
+              atomicAdd(w, (uint32_t)edge_count(wv[c]) << ((post & 1) * 16));
+            } else {
+              atomicAdd(dst + post, edge_count(wv[c]));
+            }
+          }
         }
       }
     }
@@ -231,6 +260,7 @@ struct Neuron {
   float v, g, r;      // membrane, conductance, refractory counter
   float keep;         // 1 - spike of the previous step
   float m_fire, m_in, m_hold, v_hold, rs;
+  float v_th;         // threshold; +inf under the fire mask (see lif_step)
   bool silenced;
 };
 
@@ -249,44 +279,62 @@ __device__ __forceinline__ float lif_step(Neuron& s, const fis_lif_params& P, in
   // membrane with the previous conductance (sim.py:936-938)
   float v = __fadd_rn(s.v, vstim);
   v = __fadd_rn(v, __fmul_rn(P.a_mem, __fsub_rn(s.g, __fsub_rn(v, P.v_rest))));
-  // hold, threshold, reset (sim.py:943-952)
+  // hold, threshold, reset (sim.py:943-952).  spikes = (v > v_th) * m_fire
+  // with m_fire in {0, 1} is +0 or 1; comparing against +inf where m_fire is
+  // 0 gives the same bits (a finite v never exceeds +inf) without the multiply.
   v = __fadd_rn(__fmul_rn(v, s.m_hold), s.v_hold);
-  const float sp = __fmul_rn((v > P.v_th) ? 1.f : 0.f, s.m_fire);
+  const bool fire = v > s.v_th;
+  const float sp = fire ? 1.f : 0.f;
   s.v = __fsub_rn(v, __fmul_rn(__fsub_rn(v, P.v_reset), sp));
   s.g = __fsub_rn(gn, __fmul_rn(gn, sp));
-  s.keep = __fsub_rn(1.f, sp);
+  s.keep = fire ? 0.f : 1.f;
   return sp;
 }
 
 // The step loop over K steps: `kDrive` selects whether any lane of the warp is
 // driven, so warps without drive carry no drive logic at all.  Returns the
 // number of spikes of this neuron (exact in float).
-template <bool kTape, bool kDrive>
+// The staged input of step k for this thread: an int32 column, or (kHalf) the
+// thread's half of a biased uint16 pair, masked to zero for silenced neurons
+// and padding lanes.
+struct Staged {
+  const int32_t* col;  // this thread's word of slot 0; slot k is kUpdThreads words further
+  int shift;           // kHalf: 16 for the high half of the pair, else 0
+  int32_t mask;        // kHalf: 0 for a silenced neuron, else all ones
+};
+
+template <bool kHalf>
+__device__ __forceinline__ int32_t staged(const Staged& s, int k) {
+  const int32_t w = s.col[k * kUpdThreads];
+  if (kHalf) return ((int32_t)(((uint32_t)w >> s.shift) & 0xFFFFu) - 0x8000) & s.mask;
+  return w;
+}
+
+template <bool kTape, bool kDrive, bool kHalf>
 __device__ __forceinline__ float step_loop(Neuron& st, const fis_engine& E, int K, int ka,
                                            int kb, bool valid, uint32_t dmask,
-                                           const int32_t (*sring)[kUpdThreads],
-                                           uint32_t* sbal, int lane, int64_t sidx) {
+                                           const Staged& in, uint32_t* sbal, int64_t sidx) {
   const float kick = E.p.kick;
   float nspk = 0.f;
+  // Every lane stores the warp's ballot word (the same value to the same
+  // address), so the store needs no lane predicate.
   if (ka == 0 && kb == K) {
-#pragma unroll 2
+    // Lanes past the last neuron run the same arithmetic on inert values
+    // (never above an infinite threshold) and store nothing.
+#pragma unroll 4
     for (int k = 0; k < K; ++k) {
-      const int32_t c_in = sring[k][threadIdx.x];
-      float sp = 0.f;
-      if (valid) {
-        float vstim = 0.f;
-        if (kTape) vstim = E.vstim[sidx];
-        else if (kDrive) vstim = ((dmask >> k) & 1u) ? kick : 0.f;
-        sp = lif_step(st, E.p, c_in, vstim);
-      }
-      const unsigned bal = __ballot_sync(0xFFFFFFFFu, sp != 0.f);
-      if (lane == 0) sbal[k] = bal;
+      const int32_t c_in = staged<kHalf>(in, k);
+      float vstim = 0.f;
+      if (kTape) vstim = valid ? E.vstim[sidx] : 0.f;
+      else if (kDrive) vstim = ((dmask >> k) & 1u) ? kick : 0.f;
+      const float sp = lif_step(st, E.p, c_in, vstim);
+      sbal[k] = __ballot_sync(0xFFFFFFFFu, sp != 0.f);
       nspk = __fadd_rn(nspk, sp);
     }
   } else {
 #pragma unroll 1
     for (int k = 0; k < K; ++k) {
-      const int32_t c_in = sring[k][threadIdx.x];
+      const int32_t c_in = staged<kHalf>(in, k);
       float sp = 0.f;
       if (valid && k >= ka && k < kb) {
         float vstim = 0.f;
@@ -294,8 +342,7 @@ __device__ __forceinline__ float step_loop(Neuron& st, const fis_engine& E, int 
         else if (kDrive) vstim = ((dmask >> k) & 1u) ? kick : 0.f;
         sp = lif_step(st, E.p, c_in, vstim);
       }
-      const unsigned bal = __ballot_sync(0xFFFFFFFFu, sp != 0.f);
-      if (lane == 0) sbal[k] = bal;
+      sbal[k] = __ballot_sync(0xFFFFFFFFu, sp != 0.f);
       nspk = __fadd_rn(nspk, sp);
     }
   }
@@ -305,16 +352,17 @@ __device__ __forceinline__ float step_loop(Neuron& st, const fis_engine& E, int 
 // Grid: one CTA per (trial of the group, tile of 256 neurons); the trial's
 // rows of the scratch ring are padded to ring_row(n), so each CTA's slice of
 // a ring slot is one aligned 1 KB line of the async bulk copy engine.
-template <bool kTape>
-__global__ void __launch_bounds__(kUpdThreads, 4)
+template <bool kTape, bool kHalf>
+__global__ void __launch_bounds__(kUpdThreads, 5)
 k_update(const fis_engine E, const int b0, const int nb, const int K,
          int32_t* __restrict__ ring, float* __restrict__ spikes_out,
          const int bump) {
   // The block's delayed input, one column per thread: staged here so the step
   // loop stays rolled (a compact body that fits the instruction cache) and can
-  // index it by step.
-  __shared__ int32_t sring[FIS_MAX_BLOCK][kUpdThreads];
-  __shared__ __align__(16) int32_t szero[kUpdThreads];             // source of the clearing
+  // index it by step.  With kHalf the staged values are the ring's biased
+  // uint16 pairs, decoded into sring in place.
+  __shared__ __align__(16) int32_t sring[FIS_MAX_BLOCK][kUpdThreads];
+  __shared__ __align__(16) uint32_t szero[kUpdThreads];            // source of the clearing
   __shared__ uint32_t sdrive[kUpdThreads];                         // kick bit per step
   __shared__ float sprob[kUpdThreads];                             // Bernoulli p per lane
   __shared__ uint32_t sbal[kUpdThreads / kWarp][FIS_MAX_BLOCK];    // raster words per step
@@ -322,21 +370,39 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
   const int L = E.p.lag;
   const int Wd = (n + kWarp - 1) / kWarp;
   const int NR = ring_row(n);
-  const int tiles = NR / kTile;
-  const int bl = blockIdx.x / tiles;
-  const int tile = blockIdx.x - bl * tiles;
+  const int bl = blockIdx.y;    // trial of the group
+  const int tile = blockIdx.x;  // 256-neuron tile
   const int i = tile * kTile + threadIdx.x;
   const int b = b0 + bl;
   const int lane = threadIdx.x & (kWarp - 1);
   const int wib = threadIdx.x / kWarp;
   const bool valid = i < n;
   const bool warp_valid = (i - lane) < n;
-  const int64_t t0 = *E.clock;
+  const fis_clock ck = *E.clock;
+  const int64_t t0 = ck.step;
   const fis_trial tr = E.trials[b];
   const int ka = (int)max((int64_t)0, min(tr.start - t0, (int64_t)K));
   const int kb = (int)max((int64_t)0, min(tr.end - t0, (int64_t)K));
   const int64_t sidx = (int64_t)b * n + i;
 
+  if (ka >= kb) {
+    // The trial does not run in this block (not started, or finished and
+    // frozen in place): only return its ring slots to empty, as scatters of
+    // its last spikes may still land there.  Uniform across the CTA.
+    if (threadIdx.x == 0) {
+      int32_t* rt = ring + (int64_t)bl * NR + tile * kTile;
+      uint16_t* rt16 = reinterpret_cast<uint16_t*>(ring) + (int64_t)bl * NR + tile * kTile;
+      for (int j = threadIdx.x; j < kTile; ++j) szero[j] = kHalf ? kEmptyPair : 0u;
+      fence_proxy_async_shared();
+      const int sst = nb * NR;
+      for (int k = 0; k < K; ++k) {
+        if (kHalf) bulk_store(rt16 + (int64_t)k * sst, szero, kTile * 2);
+        else bulk_store(rt + (int64_t)k * sst, szero, kTile * 4);
+      }
+      bulk_commit();
+      bulk_wait_all();
+    }
+  } else {
   uint32_t fl = 0;
   float rate = 0.f;
   Neuron st;
@@ -352,10 +418,24 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
 
   // Stage the delayed input of the K steps with asynchronous copies (no
   // registers held, all K requests in flight at once).  A silenced neuron has
-  // no incoming synapses (sim.py:324-336): it stages zeros.
-  const int sstride = nb * NR;  // < 2**31 / FIS_MAX_BLOCK, checked on the host
-  int32_t* rtile = ring + (int64_t)bl * NR + tile * kTile;
-  {
+  // no incoming synapses (sim.py:324-336): it reads as zero.
+  const int sstride = nb * NR;  // elements; < 2**31 / FIS_MAX_BLOCK, checked on the host
+  int32_t* rtile = ring + (int64_t)bl * NR + tile * kTile;                 // int32 ring
+  uint16_t* rtile16 = reinterpret_cast<uint16_t*>(ring) + (int64_t)bl * NR + tile * kTile;
+  if (kHalf) {
+    // 512 bytes per slot: the first 128 threads copy one word (two neurons)
+    // each; the words land in the first half of sring[k] and are decoded
+    // below, after the copies complete.
+    if (threadIdx.x < kTile / 2) {
+      const uint16_t* src = rtile16 + 2 * threadIdx.x;
+#pragma unroll 4
+      for (int k = 0; k < K; ++k) {
+        cp_async4(&sring[k][threadIdx.x], src);
+        src += sstride;
+      }
+    }
+    szero[threadIdx.x] = kEmptyPair;
+  } else {
     const int32_t* src = rtile + threadIdx.x;
     const bool load = valid && !st.silenced;
 #pragma unroll 4
@@ -364,17 +444,18 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
       else sring[k][threadIdx.x] = 0;
       src += sstride;
     }
+    szero[threadIdx.x] = 0u;
   }
-  szero[threadIdx.x] = 0;
 
-  const int slot0 = (int)mod_pos(t0, L);  // ring-of-lists slot of step t0
+  const int slot0 = ck.slot;  // ring-of-lists slot of step t0
   // this warp's raster words, one per slot: bits[b][word][slot]
   uint32_t* bitrow = E.bits + ((int64_t)b * Wd + (i >> 5)) * L;
   bool s_prev = false;
   if (warp_valid && t0 - 1 >= tr.start && t0 >= 1)
     s_prev = (bitrow[slot0 == 0 ? L - 1 : slot0 - 1] >> lane) & 1u;
   st.keep = s_prev ? 0.f : 1.f;
-  st.m_fire = (fl & FIS_FL_FIRE_OFF) ? 0.f : 1.f;
+  st.m_fire = (!valid || (fl & FIS_FL_FIRE_OFF)) ? 0.f : 1.f;
+  st.v_th = st.m_fire != 0.f ? E.p.v_th : __int_as_float(0x7f800000);
   st.m_in = (fl & FIS_FL_IN_OFF) ? 0.f : 1.f;
   const bool hold = fl & FIS_FL_HOLD;
   st.m_hold = hold ? 0.f : 1.f;
@@ -382,6 +463,24 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
   st.rs = (fl & FIS_FL_NOREFRAC) ? 0.f : E.p.refrac_steps;
   const int64_t own0 = t0 - tr.start;  // the trial's own step at k = 0
 
+  // All staged copies are in shared memory: return the consumed ring slots to
+  // empty with one bulk copy per slot, so the scratch ring needs no clearing
+  // pass and the step loop no stores.
+  cp_async_wait_all();
+  fence_proxy_async_shared();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (kHalf) {
+      for (int k = 0; k < K; ++k) bulk_store(rtile16 + (int64_t)k * sstride, szero, kTile * 2);
+    } else {
+      for (int k = 0; k < K; ++k) bulk_store(rtile + (int64_t)k * sstride, szero, kTile * 4);
+    }
+    bulk_commit();
+  }
+
+
+  // Every lane of a warp runs the same loop (the choice depends on the trial
+  // and on the warp's ballot only), so every lane reaches each ballot.
   // Poisson drive of the whole block (sim.py:859-861), before the step loop:
   // draw j of neuron i is word j % 4 of Philox4x32-10 at counter
   // (i, j / 4, trial lane); the (neuron, quad) pairs of the warp's driven
@@ -425,26 +524,21 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
     }
   }
 
-  // All staged copies are in shared memory: return the consumed ring slots to
-  // zero with one bulk copy per slot, so the scratch ring needs no clearing
-  // pass and the step loop no stores.
-  cp_async_wait_all();
-  fence_proxy_async_shared();
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    for (int k = 0; k < K; ++k) bulk_store(rtile + (int64_t)k * sstride, szero, kTile * 4);
-    bulk_commit();
-  }
-
-  // Every lane of a warp runs the same loop (the choice depends on the trial
-  // and on the warp's ballot only), so every lane reaches each ballot.
+  // The barrier above also orders every thread's staged copies before the
+  // loop (with kHalf a thread reads its neighbour's word too).  The drive
+  // precompute runs after it, so warps without driven neurons do not wait
+  // for those that have.
+  Staged in;
+  in.col = kHalf ? &sring[0][threadIdx.x >> 1] : &sring[0][threadIdx.x];
+  in.shift = (threadIdx.x & 1) * 16;
+  in.mask = (valid && !st.silenced) ? -1 : 0;
   float nspk;
   if (kTape)
-    nspk = step_loop<true, false>(st, E, K, ka, kb, valid, 0u, sring, sbal[wib], lane, sidx);
+    nspk = step_loop<true, false, kHalf>(st, E, K, ka, kb, valid, 0u, in, sbal[wib], sidx);
   else if (warp_driven)
-    nspk = step_loop<false, true>(st, E, K, ka, kb, valid, dmask, sring, sbal[wib], lane, sidx);
+    nspk = step_loop<false, true, kHalf>(st, E, K, ka, kb, valid, dmask, in, sbal[wib], sidx);
   else
-    nspk = step_loop<false, false>(st, E, K, ka, kb, valid, 0u, sring, sbal[wib], lane, sidx);
+    nspk = step_loop<false, false, kHalf>(st, E, K, ka, kb, valid, 0u, in, sbal[wib], sidx);
   __syncwarp();
   // the raster words of the K steps into the ring of the last L steps
   if (lane < K && warp_valid) {
@@ -465,7 +559,7 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
     const int B = E.batch;
     const bool out_on = !(fl & (FIS_FL_OUT_OFF | FIS_FL_SILENCED));
     const int nch = E.nchunks[i];
-    const int slot20 = (int)mod_pos(t0, 2 * L);
+    const int slot20 = ck.slot2;
     for (int k = 0; k < K; ++k) {
       if (!((sbal[wib][k] >> lane) & 1u)) continue;
       const int sl = slot0 + k < L ? slot0 + k : slot0 + k - L;
@@ -477,7 +571,9 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
           if (pos + q < E.list_cap) dst[pos + q] = ((uint32_t)i << 8) | (uint32_t)q;
       }
       if (tr.rec >= 0 && tr.rec < E.n_recs && tr.bin_steps > 0) {
-        const int64_t bin = (own0 + k) / tr.bin_steps;
+        const int64_t own = own0 + k;
+        const int64_t bin = own < 0x7FFFFFFF ? (int64_t)((int)own / tr.bin_steps)
+                                              : own / tr.bin_steps;
         if (bin < tr.n_bins) atomicAdd(E.recs[tr.rec] + bin * n + i, 1);
       }
     }
@@ -486,15 +582,20 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
   // The clearing copies complete before the CTA ends (szero must stay valid
   // while they read it, and the next scatter adds into these lines).
   if (threadIdx.x == 0) bulk_wait_all();
+  }  // the trial runs in this block
 
   if (bump) {
     __syncthreads();
     if (threadIdx.x == 0) {
       __threadfence();
       const unsigned prev = atomicAdd(E.done, 1u);
-      if (prev == gridDim.x - 1) {
+      if (prev == gridDim.x * gridDim.y - 1) {
         *E.done = 0u;
-        *E.clock = t0 + K;
+        fis_clock next;
+        next.step = t0 + K;
+        next.slot = wrap(ck.slot + K, L);
+        next.slot2 = wrap(ck.slot2 + K, 2 * L);
+        *E.clock = next;
         __threadfence();
       }
     }
@@ -525,7 +626,7 @@ __global__ void k_ring_to_f32(const fis_engine E, int b0, int nb,
 
 __global__ void k_spikes_f32(const fis_engine E, int b0, int nb, int64_t step,
                              float* __restrict__ out) {
-  const int n = E.n, B = E.batch, L = E.p.lag;
+  const int n = E.n, L = E.p.lag;
   const int Wd = (n + kWarp - 1) / kWarp;
   const int64_t total = (int64_t)nb * n;
   for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < total;
@@ -540,7 +641,9 @@ __global__ void k_load_spikes(const fis_engine E, int b0, int nb,
                               const float* __restrict__ sp) {
   const int n = E.n, B = E.batch, L = E.p.lag;
   const int Wd = (n + kWarp - 1) / kWarp;
-  const int64_t u = *E.clock - 1;
+  const fis_clock ck = *E.clock;
+  const int64_t u = ck.step - 1;
+  const int su = wrap(ck.slot + L - 1, L), su2 = wrap(ck.slot2 + 2 * L - 1, 2 * L);
   const int64_t npad = (int64_t)Wd * kWarp;
   const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (u < 0 || gid >= (int64_t)nb * npad) return;
@@ -549,21 +652,24 @@ __global__ void k_load_spikes(const fis_engine E, int b0, int nb,
   const int b = b0 + bl;
   const bool fired = i < n && sp[(int64_t)bl * n + i] != 0.f;
   const unsigned bal = __ballot_sync(0xFFFFFFFFu, fired);
-  if ((threadIdx.x & 31) == 0) E.bits[((int64_t)b * Wd + (i >> 5)) * L + mod_pos(u, L)] = bal;
+  if ((threadIdx.x & 31) == 0) E.bits[((int64_t)b * Wd + (i >> 5)) * L + su] = bal;
   if (fired) {
     const int nch = E.nchunks[i];
     if (nch > 0) {
-      const int32_t pos = atomicAdd(E.list_len + mod_pos(u, 2 * L) * B + b, nch);
-      uint32_t* dst = E.lists + ((int64_t)mod_pos(u, L) * B + b) * E.list_cap;
+      const int32_t pos = atomicAdd(E.list_len + (int64_t)su2 * B + b, nch);
+      uint32_t* dst = E.lists + ((int64_t)su * B + b) * E.list_cap;
       for (int q = 0; q < nch; ++q)
         if (pos + q < E.list_cap) dst[pos + q] = ((uint32_t)i << 8) | (uint32_t)q;
     }
   }
 }
 
-// dst[r][b][i] += src[r][b][i] with separate row and trial strides.
+// dst[r][b][i] += src[r][b][i] with separate row and trial strides; with
+// `half` the destination is the biased uint16 ring (each element is written
+// by one thread only, so a plain 16-bit add is exact).
 __global__ void k_add_rows(int n, int nb, int rows, const int32_t* __restrict__ src, int64_t ss,
-                           int64_t st, int32_t* __restrict__ dst, int64_t ds, int64_t dt) {
+                           int64_t st, int32_t* __restrict__ dst, int64_t ds, int64_t dt,
+                           int half) {
   const int64_t total = (int64_t)rows * nb * n;
   for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < total;
        x += (int64_t)gridDim.x * blockDim.x) {
@@ -571,8 +677,20 @@ __global__ void k_add_rows(int n, int nb, int rows, const int32_t* __restrict__ 
     const int64_t rb = x / n;
     const int bb = (int)(rb % nb);
     const int64_t r = rb / nb;
-    dst[r * ds + bb * dt + i] += src[r * ss + bb * st + i];
+    const int32_t v = src[r * ss + bb * st + i];
+    if (half) {
+      uint16_t* d = reinterpret_cast<uint16_t*>(dst) + r * ds + bb * dt + i;
+      *d = (uint16_t)(*d + (uint16_t)v);
+    } else {
+      dst[r * ds + bb * dt + i] += v;
+    }
   }
+}
+
+__global__ void k_fill32(uint32_t* __restrict__ dst, int64_t words, uint32_t value) {
+  for (int64_t x = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; x < words;
+       x += (int64_t)gridDim.x * blockDim.x)
+    dst[x] = value;
 }
 
 int launch_status() {
@@ -650,6 +768,7 @@ int fis_scatter(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, in
   A.filter_last = 1;
   A.ring = ring;
   A.trial_stride = ring_row(e->n);
+  A.half = e->ring16 ? 1 : 0;
   const size_t smem = sizeof(int32_t) * (size_t)((k_steps + 1) * nb + 1);
   k_scatter<<<sm_count() * 4, kScatThreads, smem, (cudaStream_t)stream>>>(*e, A);
   return launch_status();
@@ -659,13 +778,20 @@ int fis_update(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, int
                float* spikes_out, int32_t last_group, void* stream) {
   const int rc = check_block(e, b0, nb, k_steps, ring);
   if (rc) return rc;
-  const int64_t ugrid = (int64_t)nb * (ring_row(e->n) / kTile);
-  if (e->vstim)
-    k_update<true><<<(unsigned)ugrid, kUpdThreads, 0, (cudaStream_t)stream>>>(
-        *e, b0, nb, k_steps, ring, spikes_out, last_group ? 1 : 0);
-  else
-    k_update<false><<<(unsigned)ugrid, kUpdThreads, 0, (cudaStream_t)stream>>>(
-        *e, b0, nb, k_steps, ring, spikes_out, last_group ? 1 : 0);
+  const dim3 ugrid(ring_row(e->n) / kTile, nb);
+  const int bump = last_group ? 1 : 0;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (e->vstim) {
+    if (e->ring16)
+      k_update<true, true><<<ugrid, kUpdThreads, 0, st>>>(*e, b0, nb, k_steps, ring, spikes_out, bump);
+    else
+      k_update<true, false><<<ugrid, kUpdThreads, 0, st>>>(*e, b0, nb, k_steps, ring, spikes_out, bump);
+  } else {
+    if (e->ring16)
+      k_update<false, true><<<ugrid, kUpdThreads, 0, st>>>(*e, b0, nb, k_steps, ring, spikes_out, bump);
+    else
+      k_update<false, false><<<ugrid, kUpdThreads, 0, st>>>(*e, b0, nb, k_steps, ring, spikes_out, bump);
+  }
   return launch_status();
 }
 
@@ -730,6 +856,7 @@ int fis_delay_buffer(const fis_engine* e, int32_t b0, int32_t nb, int32_t* scrat
   A.filter_last = 0;
   A.ring = scratch;
   A.trial_stride = e->n;
+  A.half = 0;  // the delay-ring scratch is int32
   const size_t smem = sizeof(int32_t) * (size_t)((R + 1) * nb + 1);
   k_scatter<<<sm_count() * 4, kScatThreads, smem, st>>>(*e, A);
   if ((rc = launch_status())) return rc;
@@ -774,7 +901,7 @@ int fis_add_rows(const fis_engine* e, int32_t nb, int32_t rows, const int32_t* s
   const int64_t total = (int64_t)rows * nb * e->n;
   k_add_rows<<<grid_for(total, 256), 256, 0, (cudaStream_t)stream>>>(
       e->n, nb, rows, src, src_row_stride, src_trial_stride, dst, dst_row_stride,
-      dst_trial_stride);
+      dst_trial_stride, e->ring16 ? 1 : 0);
   return launch_status();
 }
 
@@ -838,11 +965,18 @@ extern "C" int fis_block_noalloc(const fis_engine* e, int32_t b0, int32_t nb, in
   int rc = fis_check(e);
   if (rc) return rc;
   if (nb < 1 || k_steps < 1) return FIS_E_BOUNDS;
-  const int64_t need = (int64_t)k_steps * nb * ring_row(e->n);
+  const int64_t elems = (int64_t)k_steps * nb * ring_row(e->n);
+  const int64_t need = e->ring16 ? elems / 2 : elems;  // 32-bit words
   if (need > (int64_t)FIS_NOALLOC_RING_INTS) return FIS_E_BOUNDS;
   int32_t* ring = nullptr;
   if ((rc = noalloc_ring(&ring))) return rc;
-  rc = (int)cudaMemsetAsync(ring, 0, sizeof(int32_t) * (size_t)need, (cudaStream_t)stream);
+  if (e->ring16) {
+    k_fill32<<<grid_for(need, 256), 256, 0, (cudaStream_t)stream>>>(
+        reinterpret_cast<uint32_t*>(ring), need, kEmptyPair);
+    rc = launch_status();
+  } else {
+    rc = (int)cudaMemsetAsync(ring, 0, sizeof(int32_t) * (size_t)need, (cudaStream_t)stream);
+  }
   if (rc) return rc;
   return fis_block(e, b0, nb, k_steps, ring, spikes_out, last_group, stream);
 }

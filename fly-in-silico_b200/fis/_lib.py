@@ -73,7 +73,8 @@ class EngineDesc(ctypes.Structure):
                 ("recs", ctypes.c_void_p), ("nnz", ctypes.c_int64),
                 ("list_cap", ctypes.c_int64), ("n", ctypes.c_int32),
                 ("batch", ctypes.c_int32), ("chunk", ctypes.c_int32),
-                ("n_recs", ctypes.c_int32), ("p", LifParams)]
+                ("n_recs", ctypes.c_int32), ("ring16", ctypes.c_int32),
+                ("pad_", ctypes.c_int32), ("p", LifParams)]
 
 
 _lib = None

@@ -69,15 +69,25 @@ def host_rows(specs, n):
 
 
 class Batch:
-    """Trial slots on one GPU; load specs, advance, read per-trial results."""
+    """Trial slots on one GPU; load specs, advance, read per-trial results.
+
+    Recording buffers (int32 [n_bins][N], one atomic add per spike inside the
+    update kernel) live in a registry: a trial records either into a buffer of
+    its own or into one shared by the trials of a request (their spikes then
+    sum, as the reference's bins sum over trials, ``sim.py:1068-1076``).
+    """
 
     def __init__(self, conn: Connectome, capacity: int, params=None, device="cuda",
-                 group=None, core: Core | None = None):
-        self.core = core or Core(conn, capacity, params=params, device=device, group=group)
+                 group=None, chunk=None, core: Core | None = None):
+        self.core = core or Core(conn, capacity, params=params, device=device, group=group,
+                                 chunk=chunk)
         self.n = self.core.n
         self.capacity = self.core.batch
-        self._recs = [None] * self.capacity
+        self._recs = {}                          # index -> int32 [n_bins][N]
+        self._rec_refs = {}                      # index -> trials recording into it
+        self._slot_rec = [None] * self.capacity  # slot -> index
         self._pinned = {}
+        self._dummy_rec = None
 
     def _staging(self, name, shape, dtype):
         buf = self._pinned.get(name)
@@ -86,12 +96,49 @@ class Batch:
             self._pinned[name] = buf
         return buf
 
-    def load(self, slots, specs, start=None):
+    # --- recording registry ---------------------------------------------------
+
+    def _rec_add(self, tensor, refs):
+        idx = 0
+        while idx in self._recs:
+            idx += 1
+        self._recs[idx] = tensor
+        self._rec_refs[idx] = refs
+        return idx
+
+    def _rec_upload(self):
+        if self._dummy_rec is None:
+            self._dummy_rec = torch.zeros((1, self.n), dtype=torch.int32, device=self.core.device)
+        top = max(self._recs) + 1 if self._recs else 0
+        self.core.set_recordings([self._recs.get(i, self._dummy_rec) for i in range(top)])
+
+    def release(self, slot):
+        """Detach ``slot`` from its recording (freed with its last trial)."""
+        idx = self._slot_rec[slot]
+        self._slot_rec[slot] = None
+        if idx is None:
+            return
+        self._rec_refs[idx] -= 1
+        if self._rec_refs[idx] <= 0:
+            del self._recs[idx]
+            del self._rec_refs[idx]
+
+    def recording(self, slot):
+        """The recording buffer of ``slot`` (device int32 [n_bins][N])."""
+        return self._recs[self._slot_rec[slot]]
+
+    def recordings(self):
+        return list(self._recs.values())
+
+    # --- trials -------------------------------------------------------------------
+
+    def load(self, slots, specs, start=None, rec=None):
         """Place ``specs`` into ``slots`` starting at global step ``start``.
 
         Rows are built on the host and copied once (pinned, asynchronous);
-        state is reset to the reference's initial values; each trial gets a
-        recording buffer int32 [n_bins][N] of its own.
+        state is reset to the reference's initial values.  ``rec``: a shared
+        recording buffer for all these trials; by default each trial gets one
+        of its own.
         """
         c = self.core
         slots = list(slots)
@@ -103,43 +150,40 @@ class Batch:
         rpin.numpy()[:] = rates
         idx = torch.as_tensor(slots, dtype=torch.long, device=c.device)
         contiguous = slots == list(range(slots[0], slots[0] + len(slots)))
+        rows = slice(slots[0], slots[0] + len(slots)) if contiguous else idx
         if contiguous:
-            c.flags[slots[0]:slots[0] + len(slots)].copy_(fpin, non_blocking=True)
-            c.rates[slots[0]:slots[0] + len(slots)].copy_(rpin, non_blocking=True)
+            c.flags[rows].copy_(fpin, non_blocking=True)
+            c.rates[rows].copy_(rpin, non_blocking=True)
         else:
             c.flags[idx] = fpin.to(c.device, non_blocking=True)
             c.rates[idx] = rpin.to(c.device, non_blocking=True)
-        for j, (b, s) in enumerate(zip(slots, specs)):
+        for b in slots:
+            if self._slot_rec[b] is not None:
+                self.release(b)
+        shared = None
+        if rec is not None:
+            shared = self._rec_add(rec, len(slots))
+        for b, s in zip(slots, specs):
             t = c.trials[b]
             t.seed = int(s.seed) & (2 ** 64 - 1)
             t.stream = 0
             t.start = start
             t.end = start + int(s.steps)
             t.v_clamp = float(np.float32(c.pdict["vReset"] if s.v_clamp is None else s.v_clamp))
-            nb = s.n_bins()
-            rec = self._recs[b]
-            if rec is None or rec.shape[0] != nb:
-                rec = torch.zeros((nb, self.n), dtype=torch.int32, device=c.device)
-                self._recs[b] = rec
+            if shared is None:
+                r = torch.zeros((s.n_bins(), self.n), dtype=torch.int32, device=c.device)
+                ri = self._rec_add(r, 1)
+                nb = s.n_bins()
             else:
-                rec.zero_()
-            t.rec = b
+                ri = shared
+                nb = int(rec.shape[0])
+            self._slot_rec[b] = ri
+            t.rec = ri
             t.bin_steps = int(s.bin_steps or max(1, s.steps))
             t.n_bins = nb
-        c.set_recordings([r if r is not None else self._dummy() for r in self._recs])
+        self._rec_upload()
         c.mark_trials()
-        c.reset_slots(idx if not contiguous else slice(slots[0], slots[0] + len(slots)))
-
-    def _dummy(self):
-        d = getattr(self, "_dummy_rec", None)
-        if d is None:
-            d = self._dummy_rec = torch.zeros((1, self.n), dtype=torch.int32,
-                                              device=self.core.device)
-        return d
-
-    def results(self, slots, out=None):
-        """Per-slot recordings (device tensors int32 [n_bins][N])."""
-        return [self._recs[b] for b in slots]
+        c.reset_slots(rows)
 
     def run(self, specs, timer=None):
         """Run ``specs`` (at most ``capacity``) to completion; host counts per trial.
@@ -156,7 +200,7 @@ class Batch:
         self.load(slots, specs)
         c.advance(max(int(s.steps) for s in specs), timer=timer)
         out = self._staging("counts", (len(specs), self.n), torch.int32)
-        dev = torch.stack([self._recs[b].sum(0, dtype=torch.int32) for b in slots])
+        dev = torch.stack([self.recording(b).sum(0, dtype=torch.int32) for b in slots])
         out.copy_(dev, non_blocking=True)
         torch.cuda.current_stream(c.device).synchronize()
         return out.numpy().copy()

@@ -22,6 +22,7 @@ from __future__ import annotations
 
 import ctypes
 import math
+import os
 
 import numpy as np
 import torch
@@ -80,7 +81,7 @@ class Core:
     """B trial slots, their state on the device, and the block launcher."""
 
     def __init__(self, conn: Connectome, batch: int, params=None, device="cuda",
-                 group=None, chunk=None, max_block=_lib.FIS_MAX_BLOCK):
+                 group=None, chunk=None, max_block=_lib.FIS_MAX_BLOCK, ring=None):
         self.device = require_cuda(device)
         self.lib = _lib.load()
         conn.check_bounds()
@@ -90,6 +91,17 @@ class Core:
                 "max |row sum| %.0f >= 2**24: integer accumulation would not be "
                 "exact for this matrix" % ex["max_abs_row_sum"])
         self.conn = conn
+        # Scratch-ring element: biased int16 when no neuron's incoming
+        # |count| sum reaches 2**15 (exact, half the ring traffic), else int32.
+        ring = ring or os.environ.get("FIS_RING", "auto")
+        if ring not in ("auto", "int16", "int32"):
+            raise ValueError("ring must be auto, int16 or int32")
+        fits16 = ex["max_abs_row_sum"] < (1 << 15)
+        if ring == "int16" and not fits16:
+            raise _lib.KernelUnavailable(
+                "an int16 ring is not exact here: max |row sum| %.0f >= 2**15"
+                % ex["max_abs_row_sum"])
+        self.ring16 = fits16 if ring == "auto" else ring == "int16"
         self.n = n = int(conn.n)
         self.batch = B = int(batch)
         if B < 1:
@@ -133,7 +145,8 @@ class Core:
             self.list_len = torch.zeros((2 * L, B), dtype=torch.int32, device=dev)
             self.words = (n + 31) // 32
             self.bits = torch.zeros((B, self.words, L), dtype=torch.int32, device=dev)
-            self.clock = torch.zeros(1, dtype=torch.int64, device=dev)
+            # fis_clock: step, then (step mod lag) | (step mod 2*lag) << 32
+            self.clock = torch.zeros(2, dtype=torch.int64, device=dev)
             self.done = torch.zeros(1, dtype=torch.int32, device=dev)
         self.trials = (_lib.Trial * B)()
         for b in range(B):
@@ -168,8 +181,17 @@ class Core:
         d.nnz = nnz
         d.list_cap = self.list_cap
         d.n, d.batch, d.chunk, d.n_recs = n, B, self.chunk, 0
+        d.ring16 = 1 if self.ring16 else 0
         d.p = self.P
         _lib.check(self.lib.fis_check(ctypes.byref(d)), "fis_check")
+
+    def set_clock(self, step):
+        """Set the device step counter (and its slot indices) and the host mirror."""
+        step = int(step)
+        L = self.lag
+        packed = (step % L) | ((step % (2 * L)) << 32)
+        self.clock.copy_(torch.tensor([step, packed], dtype=torch.int64))
+        self.step = step
 
     # --- configuration ---------------------------------------------------
 
@@ -180,8 +202,12 @@ class Core:
         self.group = int(max(1, min(int(group), self.batch)))
         self.ring_row = int(self.lib.fis_ring_row(self.n))
         with torch.cuda.device(self.device):
-            self.ring = torch.zeros((self.max_block, self.group, self.ring_row),
-                                    dtype=torch.int32, device=self.device)
+            if self.ring16:   # empty = 0x8000 (biased zero)
+                self.ring = torch.full((self.max_block, self.group, self.ring_row), -32768,
+                                       dtype=torch.int16, device=self.device)
+            else:
+                self.ring = torch.zeros((self.max_block, self.group, self.ring_row),
+                                        dtype=torch.int32, device=self.device)
 
     def set_recordings(self, bufs):
         """Recording buffers, each int32 [n_bins][N]; trials point at them by index."""
@@ -222,9 +248,12 @@ class Core:
 
     # --- stepping ------------------------------------------------------------
 
-    def block(self, k, spikes_out=None, stream=None, timer=None):
+    def block(self, k, spikes_out=None, stream=None, timer=None, rows=None):
         """Advance every slot by ``k`` steps (1 <= k <= max_block).
 
+        ``rows``: launch only the trial groups covering slots [0, rows); the
+        caller guarantees that no slot at or above it is running (a slot that
+        is launched again later is re-initialised first, see reset_slots).
         ``timer`` (optional) is called as ``timer(stream, True)`` right before
         and ``timer(stream, False)`` right after each update launch, so a caller
         can bracket the dominant kernel with CUDA events.
@@ -235,7 +264,8 @@ class Core:
         self._sync_trials()
         st = (stream or torch.cuda.current_stream(self.device)).cuda_stream
         sp = ctypes.c_void_p(spikes_out.data_ptr()) if spikes_out is not None else None
-        B, G = self.batch, self.group
+        G = self.group
+        B = self.batch if rows is None else max(1, min(int(rows), self.batch))
         for g0 in range(0, B, G):
             nb = min(G, B - g0)
             if self.pending is not None:
@@ -266,7 +296,8 @@ class Core:
         # the kernel's ring for this group is [k][nb][NR]
         rc = self.lib.fis_add_rows(ctypes.byref(self.desc), nb, hi - lo,
                                    ctypes.c_void_p(src.data_ptr()), self.batch * n, n,
-                                   ctypes.c_void_p(self.ring.data_ptr() + (lo - t0) * nb * NR * 4),
+                                   ctypes.c_void_p(self.ring.data_ptr()
+                                                   + (lo - t0) * nb * NR * self.ring.element_size()),
                                    nb * NR, NR, ctypes.c_void_p(st))
         _lib.check(rc, "fis_add_rows")
 
@@ -356,8 +387,7 @@ class Core:
         spikes of step ``step - 1`` and are queued for delivery.
         """
         step = int(step)
-        self.clock.fill_(step)
-        self.step = step
+        self.set_clock(step)
         for dst, src in ((self.v, v), (self.g, g), (self.refrac, refrac)):
             if src is not None:
                 dst.copy_(src)

@@ -242,7 +242,7 @@ class Engine:
     MASK_TENSORS = ("m_fire", "m_out", "m_in", "m_hold", "v_hold")
 
     def __init__(self, weights, n, params=None, device="cuda", batch=1, seed=0,
-                 no_refractory=None, spmv=None, allow_inexact=False, group=None):
+                 no_refractory=None, spmv=None, allow_inexact=False, group=None, ring=None):
         p = dict(params or MODEL_PARAMS)
         self.p = p
         self.n = int(n)
@@ -269,7 +269,7 @@ class Engine:
         self._conn = conn
         self._exact = conn.exactness()
         try:
-            self.core = Core(conn, self.batch, params=p, device=dev, group=group)
+            self.core = Core(conn, self.batch, params=p, device=dev, group=group, ring=ring)
         except _lib.KernelUnavailable as exc:
             raise evspmv.EventKernelUnavailable(str(exc)) from exc
         c = self.core
@@ -362,7 +362,9 @@ class Engine:
             "побитовое равенство обеспечено": bool(self._exact["ok"]),
             "условия равенства": evspmv.exactness_from(self._exact),
             "сборка ядра": {"библиотека": str(_lib.LIB_PATH.name), "abi": _lib.FIS_ABI_VERSION,
-                            "цель": "sm_100a", "кольцо": "int32, блок до 20 шагов",
+                            "цель": "sm_100a",
+                            "кольцо": ("int16 со смещением" if self.core.ring16 else "int32")
+                            + ", блок до 20 шагов",
                             "группа проб": self.core.group},
         }
 
@@ -472,6 +474,40 @@ class Engine:
             c.desc.vstim = None
         self._spikes_version = self.spikes._version
         return self.spikes
+
+    def run_block(self, rates, steps):
+        """``steps`` ticks at constant ``rates``; returns the summed spikes [B, N].
+
+        The closed loop's brain step (``body.py:1908-1912``: ``acc +=
+        engine.step(rates)[0]`` 200 times per 20 ms control step) as one call:
+        the steps run in 20-step fused blocks and the spikes are summed on the
+        device by the update kernel, with no host work between steps.  Equal to
+        stepping one by one; ``spikes`` holds the last step afterwards.
+        """
+        self._check_spikes_untouched()
+        c = self.core
+        r = self._rates_arg(rates)
+        steps = int(steps)
+        acc = torch.zeros((self.batch, self.n), dtype=torch.int32, device=c.device)
+        saved = [(c.trials[b].rec, c.trials[b].bin_steps, c.trials[b].n_bins)
+                 for b in range(self.batch)]
+        recs, n_recs = c.recs, c.desc.n_recs
+        c.set_recordings([acc[b:b + 1] for b in range(self.batch)])
+        for b in range(self.batch):
+            c.trials[b].rec, c.trials[b].bin_steps, c.trials[b].n_bins = b, 0x7FFFFFFF, 1
+        c.mark_trials()
+        c.desc.rates = r.data_ptr()
+        try:
+            c.advance(steps, spikes_out=self.spikes)
+        finally:
+            c.desc.rates = c.rates.data_ptr()
+            for b, (rec, bs, nb) in enumerate(saved):
+                c.trials[b].rec, c.trials[b].bin_steps, c.trials[b].n_bins = rec, bs, nb
+            c.mark_trials()
+            c.set_recordings(recs)
+        self.calls += steps
+        self._spikes_version = self.spikes._version
+        return acc.to(torch.float32)
 
     def use_graphs(self, enable=True):
         """Capture the step into a CUDA graph (sim.py:634-743)."""
@@ -612,7 +648,7 @@ class Engine:
 
 def build_engine(weights=None, neurons=None, silenced=None, params=None, device=None,
                  batch=1, seed=0, no_refractory=None, graphs=True, spmv=None,
-                 allow_inexact=False, group=None):
+                 allow_inexact=False, group=None, ring=None):
     """Return a ready :class:`Engine` (sim.py:956-987).
 
     ``weights`` is the reference's sparse ``W[post, pre]`` or a
@@ -630,7 +666,7 @@ def build_engine(weights=None, neurons=None, silenced=None, params=None, device=
     conn = conn.without(sil)
     eng = Engine(conn, n, params=params, device=device or "cuda", batch=batch, seed=seed,
                  no_refractory=no_refractory, spmv=spmv, allow_inexact=allow_inexact,
-                 group=group)
+                 group=group, ring=ring)
     if graphs:
         eng.use_graphs()
     return eng

@@ -69,6 +69,15 @@ typedef struct fis_lif_params {
   int32_t pad_;
 } fis_lif_params;
 
+/* The device-side step counter.  `slot` and `slot2` are step mod lag and
+ * step mod 2*lag, kept beside the step so kernels index the spike history
+ * without 64-bit division; kernels advance all three together. */
+typedef struct fis_clock {
+  int64_t step;
+  int32_t slot;
+  int32_t slot2;
+} fis_clock;
+
 /* One trial slot.  Times are global engine steps. */
 typedef struct fis_trial {
   uint64_t seed;      /* Philox key of this trial's Poisson drive            */
@@ -99,7 +108,7 @@ typedef struct fis_trial {
  *   lists    uint32 [L][B][list_cap]  spike entries pre << 8 | chunk
  *   list_len int32 [2L][B]     entries per (step mod 2L, trial)
  *   bits     uint32 [B][W][L]  spike raster of the last L steps (slot innermost)
- *   clock    int64 [1]         global steps completed (device-side)
+ *   clock    fis_clock [1]     global steps completed (device-side)
  *   done     uint32 [1]        block-completion counter, zero between calls
  *   recs     int32* [n_recs]   recording buffers [n_bins][N]
  */
@@ -117,7 +126,7 @@ typedef struct fis_engine {
   uint32_t* lists;
   int32_t* list_len;
   uint32_t* bits;
-  int64_t* clock;
+  fis_clock* clock;
   uint32_t* done;
   int32_t* const* recs;
   int64_t nnz;
@@ -126,6 +135,8 @@ typedef struct fis_engine {
   int32_t batch;
   int32_t chunk;      /* edges per scatter work item, a multiple of 128     */
   int32_t n_recs;
+  int32_t ring16;     /* scratch ring of biased int16 counts (see below)    */
+  int32_t pad_;
   fis_lif_params p;
 } fis_engine;
 
@@ -170,9 +181,14 @@ int fis_check(const fis_engine* e);
  * k_steps steps (refractory gate, delayed input, conductance, Poisson drive,
  * membrane, hold, threshold, reset).  Replaces one call of Engine.step per
  * step (sim.py:745-771, 863-953).
- *   ring        int32 [k_steps][nb][NR], NR = fis_ring_row(N) (N rounded up
- *               to a multiple of 256), 16-byte aligned; all zero on entry,
- *               all zero on exit
+ *   ring        [k_steps][nb][NR], NR = fis_ring_row(N) (N rounded up to a
+ *               multiple of 256), 16-byte aligned; "empty" on entry and on
+ *               exit.  Elements are int32 counts (empty = 0), or, when
+ *               e->ring16 is set, uint16 values 0x8000 + count (empty =
+ *               0x8000): exact whenever every neuron's sum of |count| over
+ *               its incoming synapses is below 2**15, as then no partial sum
+ *               leaves (-2**15, 2**15) and a 32-bit atomic add on a pair of
+ *               neighbours never carries across the halves
  *   spikes_out  float [B][N] or NULL: the spikes of the block's last step
  *   last_group  nonzero when this call completes the block for all trial
  *               groups; the device clock then advances by k_steps

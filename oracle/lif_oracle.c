@@ -331,4 +331,82 @@ int oracle_run(void* h, const oracle_params* p, int batch, int steps, int mode, 
   return 0;
 }
 
+/*
+ * The same equations in float64, for the error statement of the float32 path:
+ * every constant is the double the reference starts from (DT/tauSyn ...
+ * before its float32 cast), every operation is rounded to double, and the
+ * drive fires on the same Philox draws (the firing decision itself is the
+ * float32 comparison of the tape, so both runs receive the same kicks).
+ * Arrays are double [B][N] (ring [B][buf_len][N]); masks and refrac_steps
+ * are the float arrays of the float32 run.
+ */
+typedef struct oracle_params64 {
+  double a_syn, a_mem, w_scale, kick, v_rest, v_reset, v_th;
+  float prob_scale;
+  int32_t buf_len;
+} oracle_params64;
+
+int oracle_run_f64(void* h, const oracle_params64* p, int batch, int steps, double* v,
+                   double* g, double* spikes, double* refrac, double* ring, int32_t* ptr,
+                   const float* rs, const float* m_fire, const float* m_out, const float* m_in,
+                   const float* m_hold, const float* v_hold, const float* rates,
+                   const uint64_t* seeds, const uint32_t* streams, int64_t* own_t,
+                   uint8_t* raster) {
+  const oracle_ctx* c = (const oracle_ctx*)h;
+  if (!c || !p || batch < 1 || steps < 0 || p->buf_len < 1) return -1;
+  const int n = c->n;
+  const int64_t bn = (int64_t)batch * n;
+  double* rec = (double*)malloc(sizeof(double) * (size_t)bn);
+  if (!rec) return -2;
+  const int nbytes = (n + 7) / 8;
+  for (int t = 0; t < steps; ++t) {
+    const int ptr0 = *ptr;
+    for (int b = 0; b < batch; ++b) {
+      const int64_t o = (int64_t)b * n;
+      for (int i = 0; i < n; ++i) rec[o + i] = 0.0;
+      for (int pre = 0; pre < n; ++pre) {
+        const double s = spikes[o + pre] * (double)m_out[o + pre];
+        if (s == 0.0) continue;
+        for (int64_t k = c->row_ptr[pre]; k < c->row_ptr[pre + 1]; ++k)
+          rec[o + c->col[k]] += (double)c->cnt[k] * s;
+      }
+      double* R = ring + (int64_t)b * p->buf_len * n;
+      for (int i = 0; i < n; ++i) {
+        const int64_t x = o + i;
+        const float fr = rates[x] * p->prob_scale;
+        double vstim = 0.0;
+        if (fr > 0.0f) {
+          const uint32_t w = drive_word(i, own_t[b], streams[b], seeds[b]);
+          if ((float)(w >> 8) * 0x1p-24f < fr) vstim = p->kick;
+        }
+        refrac[x] = (refrac[x] + 1.0) * (1.0 - spikes[x]);
+        const double gate = (refrac[x] >= (double)rs[x]) ? 1.0 : 0.0;
+        const double delayed = R[(int64_t)ptr0 * n + i] * (double)m_in[x];
+        const double gn = g[x] * p->a_syn + delayed * gate;
+        R[(int64_t)ptr0 * n + i] = p->w_scale * rec[x];
+        double vv = v[x] + vstim;
+        vv = vv + p->a_mem * (g[x] - (vv - p->v_rest));
+        vv = vv * (double)m_hold[x] + (double)v_hold[x];
+        const double s = ((vv > p->v_th) ? 1.0 : 0.0) * (double)m_fire[x];
+        vv = vv - (vv - p->v_reset) * s;
+        v[x] = vv;
+        spikes[x] = s;
+        g[x] = gn - gn * s;
+      }
+    }
+    *ptr = (ptr0 + 1) % p->buf_len;
+    for (int b = 0; b < batch; ++b) own_t[b] += 1;
+    if (raster) {
+      uint8_t* row = raster + (int64_t)t * batch * nbytes;
+      memset(row, 0, (size_t)batch * nbytes);
+      for (int b = 0; b < batch; ++b)
+        for (int i = 0; i < n; ++i)
+          if (spikes[(int64_t)b * n + i] != 0.0)
+            row[(int64_t)b * nbytes + (i >> 3)] |= (uint8_t)(1u << (i & 7));
+    }
+  }
+  free(rec);
+  return 0;
+}
+
 int oracle_abi(void) { return 1; }

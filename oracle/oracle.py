@@ -57,6 +57,24 @@ def params(p=None) -> OracleParams:
         buf_len=buf_len, lag=buf_len + 1, pad_=0)
 
 
+class OracleParams64(ctypes.Structure):
+    _fields_ = [("a_syn", ctypes.c_double), ("a_mem", ctypes.c_double),
+                ("w_scale", ctypes.c_double), ("kick", ctypes.c_double),
+                ("v_rest", ctypes.c_double), ("v_reset", ctypes.c_double),
+                ("v_th", ctypes.c_double), ("prob_scale", ctypes.c_float),
+                ("buf_len", ctypes.c_int32)]
+
+
+def params64(p=None) -> OracleParams64:
+    """The same constants in float64, before the reference's float32 cast."""
+    p = dict(MODEL_PARAMS if p is None else p)
+    return OracleParams64(
+        a_syn=1.0 - DT / p["tauSyn"], a_mem=DT / p["tauMem"], w_scale=float(p["wScale"]),
+        kick=float(p["wScale"]) * float(p["scalePoisson"]), v_rest=float(p["vRest"]),
+        v_reset=float(p["vReset"]), v_th=float(p["vThreshold"]),
+        prob_scale=float(np.float32(DT / 1000.0)), buf_len=int(p["tDelay"] / DT) + 1)
+
+
 def build(force=False):
     """Compile the oracle with its Makefile (gcc, seconds)."""
     if LIB.exists() and not force and LIB.stat().st_mtime >= (HERE / "lif_oracle.c").stat().st_mtime:
@@ -84,6 +102,7 @@ def lib():
         L.oracle_core.argtypes = [P, P, ctypes.c_int, ctypes.c_int] + [P] * 14 + [ctypes.c_int]
         L.oracle_run.argtypes = ([P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int]
                                  + [P] * 17 + [ctypes.c_int])
+        L.oracle_run_f64.argtypes = [P, P, ctypes.c_int, ctypes.c_int] + [P] * 17
         _lib = L
     return _lib
 
@@ -189,8 +208,16 @@ class Oracle:
                 _p(self.m_fire), _p(self.m_out), _p(self.m_in), _p(self.m_hold),
                 _p(self.v_hold)]
 
+    def _threads(self, threads):
+        """Explicit count, else one thread below a million neuron-trials (the
+        per-step parallel regions cost more than they save there)."""
+        if threads:
+            return int(threads)
+        return 1 if self.batch * self.n < (1 << 20) else nthreads_default()
+
     def core(self, vstim, mode=EVENT, threads=0):
         """One ``Engine._core(voltage_stim)`` call with an explicit tape."""
+        threads = self._threads(threads)
         vstim = np.ascontiguousarray(vstim, dtype=np.float32)
         rc = lib().oracle_core(self._h, ctypes.byref(self.P), self.batch, mode,
                                *self._args(), _p(vstim), _p(self._rec), threads)
@@ -204,6 +231,7 @@ class Oracle:
         Returns the raster as uint8 bits [steps, B, ceil(N/8)] (little bit
         order) when ``raster`` is true.
         """
+        threads = self._threads(threads)
         nbytes = (self.n + 7) // 8
         out = np.zeros((steps, self.batch, nbytes), dtype=np.uint8) if raster else None
         rc = lib().oracle_run(
@@ -212,6 +240,34 @@ class Oracle:
             _p(out) if raster else None, threads)
         if rc:
             raise RuntimeError("oracle_run returned %d" % rc)
+        return out
+
+    def run_f64(self, steps, raster=False):
+        """``steps`` steps of the same equations in float64 from the current state.
+
+        Works on float64 copies (``v64``, ``g64`` ... created on first use from
+        the float32 state) and leaves the float32 state alone; the drive uses
+        the same draws, so both runs see the same kicks.
+        """
+        if not hasattr(self, "v64"):
+            self.v64 = self.v.astype(np.float64)
+            self.g64 = self.conductance.astype(np.float64)
+            self.spikes64 = self.spikes.astype(np.float64)
+            self.refrac64 = self.refrac.astype(np.float64)
+            self.ring64 = self.delay_buffer.astype(np.float64)
+            self.ptr64 = self.ptr.copy()
+            self.own64 = self.own_t.copy()
+        nbytes = (self.n + 7) // 8
+        out = np.zeros((steps, self.batch, nbytes), dtype=np.uint8) if raster else None
+        P64 = params64(self.pdict)
+        rc = lib().oracle_run_f64(
+            self._h, ctypes.byref(P64), self.batch, int(steps), _p(self.v64), _p(self.g64),
+            _p(self.spikes64), _p(self.refrac64), _p(self.ring64), _p(self.ptr64),
+            _p(self.refrac_steps), _p(self.m_fire), _p(self.m_out), _p(self.m_in),
+            _p(self.m_hold), _p(self.v_hold), _p(self.rates), _p(self.seeds), _p(self.streams),
+            _p(self.own64), _p(out) if raster else None)
+        if rc:
+            raise RuntimeError("oracle_run_f64 returned %d" % rc)
         return out
 
     @classmethod

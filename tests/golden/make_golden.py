@@ -96,11 +96,14 @@ def run_reference(name):
                    spikes=eng.spikes.numpy(), ring=eng.delay_buffer.numpy(),
                    ptr=np.int64(eng.ptr))
     else:
-        # full size: the raster as (step, trial, neuron) triples (it is sparse)
-        st, b, i = np.nonzero(np.unpackbits(raster, axis=2, bitorder="little")[:, :, :n])
+        # full size: the raster as (step, trial, neuron) triples (it is sparse),
+        # the first 1,000 steps of it for long runs, plus per-neuron counts
+        bits = np.unpackbits(raster, axis=2, bitorder="little")[:, :, :n]
+        st, b, i = np.nonzero(bits[:1000])
         out.pop("raster_bits")
         out.update(spike_step=st.astype(np.int32), spike_trial=b.astype(np.int16),
-                   spike_neuron=i.astype(np.int32))
+                   spike_neuron=i.astype(np.int32),
+                   counts=bits.sum(0).astype(np.int32))
     path = OUT / ("%s.npz" % name)
     np.savez_compressed(path, **out)
     print("%-14s %5d steps, %6d spikes, reference %.1f ms/step -> %s (%d KB)"

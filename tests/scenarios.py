@@ -42,6 +42,10 @@ SCENARIOS = {
     "full_cfg0": dict(n=138_639, e=15_091_983, conn_seed=0, batch=1, steps=1000,
                       seed=0, drive_k=2249, drive_seed=1, rates=[150.0], plan=[],
                       params=None),
+    # The same configuration over 1 s (10,000 steps): rates over the run.
+    "full_cfg0_1s": dict(n=138_639, e=15_091_983, conn_seed=0, batch=1, steps=10_000,
+                         seed=0, drive_k=2249, drive_seed=1, rates=[150.0], plan=[],
+                         params=None),
 }
 
 MILESTONES = (1, 10, 19, 20, 21, 40, 100, 200, 300, 400, 500, 1000)

