@@ -326,6 +326,7 @@ def main():
         end.record()
         barrier()
     ms = max_over_ranks(start.elapsed_time(end))
+    core.check_errors()
     clocks = sampler.summary()
     durs = []
     for evs in events:

@@ -43,16 +43,6 @@ constexpr int kScatThreads = 256;
 constexpr int kScatWarps = kScatThreads / kWarp;
 constexpr int kMaxLists = 11264;  // prefix entries in dynamic shared memory (44 KB)
 
-// 4-byte asynchronous global -> shared copy (sm_80+ cp.async), completed by
-// cp_async_wait_all() in the issuing thread.
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.wait_all;\n" ::: "memory");
-}
-
 // Bulk asynchronous shared -> global copy (sm_90+ cp.async.bulk, the TMA
 // engine): both addresses 16-byte aligned, size a multiple of 16.
 __device__ __forceinline__ void bulk_store(void* gmem, const void* smem, unsigned bytes) {
@@ -78,6 +68,50 @@ __device__ __forceinline__ int wrap(int x, int m) {
   while (x >= m) x -= m;
   return x;
 }
+
+// mbarrier and bulk (TMA) loads into shared memory.
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;\n" ::"r"(
+                   smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// Bulk copy global -> shared, completing `bytes` transactions on `bar`.
+__device__ __forceinline__ void bulk_load(void* smem, const void* gmem, unsigned bytes,
+                                          uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::
+          "r"(smem_addr(smem)),
+      "l"(gmem), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+// Wait for phase `parity` of `bar`, giving up after `limit` polls (each poll
+// may suspend the thread briefly).  Returns whether the phase completed.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, unsigned limit) {
+  const unsigned a = smem_addr(bar);
+  for (unsigned it = 0; it < limit; ++it) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+constexpr unsigned kWaitPolls = 1u << 22;   // far beyond any copy's latency
 
 // Ring rows are padded per trial to a whole number of update tiles.
 constexpr int kTile = 256;
@@ -307,7 +341,7 @@ template <bool kHalf>
 __device__ __forceinline__ int32_t staged(const Staged& s, int k) {
   const int32_t w = s.col[k * kUpdThreads];
   if (kHalf) return ((int32_t)(((uint32_t)w >> s.shift) & 0xFFFFu) - 0x8000) & s.mask;
-  return w;
+  return w & s.mask;
 }
 
 template <bool kTape, bool kDrive, bool kHalf>
@@ -315,6 +349,9 @@ __device__ __forceinline__ float step_loop(Neuron& st, const fis_engine& E, int 
                                            int kb, bool valid, uint32_t dmask,
                                            const Staged& in, uint32_t* sbal, int64_t sidx) {
   const float kick = E.p.kick;
+  // fired steps as bits, the latest step lowest: m = 2 m + spike per step, an
+  // exact float of at most 20 bits (bookkeeping, not model state, so one fused
+  // multiply-add is fine here)
   float nspk = 0.f;
   // Every lane stores the warp's ballot word (the same value to the same
   // address), so the store needs no lane predicate.
@@ -329,7 +366,7 @@ __device__ __forceinline__ float step_loop(Neuron& st, const fis_engine& E, int 
       else if (kDrive) vstim = ((dmask >> k) & 1u) ? kick : 0.f;
       const float sp = lif_step(st, E.p, c_in, vstim);
       sbal[k] = __ballot_sync(0xFFFFFFFFu, sp != 0.f);
-      nspk = __fadd_rn(nspk, sp);
+      nspk = __fmaf_rn(nspk, 2.f, sp);
     }
   } else {
 #pragma unroll 1
@@ -343,7 +380,7 @@ __device__ __forceinline__ float step_loop(Neuron& st, const fis_engine& E, int 
         sp = lif_step(st, E.p, c_in, vstim);
       }
       sbal[k] = __ballot_sync(0xFFFFFFFFu, sp != 0.f);
-      nspk = __fadd_rn(nspk, sp);
+      nspk = __fmaf_rn(nspk, 2.f, sp);
     }
   }
   return nspk;
@@ -366,6 +403,7 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
   __shared__ uint32_t sdrive[kUpdThreads];                         // kick bit per step
   __shared__ float sprob[kUpdThreads];                             // Bernoulli p per lane
   __shared__ uint32_t sbal[kUpdThreads / kWarp][FIS_MAX_BLOCK];    // raster words per step
+  __shared__ __align__(8) uint64_t sbar;                           // staging barrier
   const int n = E.n;
   const int L = E.p.lag;
   const int Wd = (n + kWarp - 1) / kWarp;
@@ -403,6 +441,11 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
       bulk_wait_all();
     }
   } else {
+  if (threadIdx.x == 0) {
+    mbar_init(&sbar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();  // the barrier exists before anyone arrives or waits
   uint32_t fl = 0;
   float rate = 0.f;
   Neuron st;
@@ -416,35 +459,22 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
   }
   st.silenced = fl & FIS_FL_SILENCED;
 
-  // Stage the delayed input of the K steps with asynchronous copies (no
-  // registers held, all K requests in flight at once).  A silenced neuron has
-  // no incoming synapses (sim.py:324-336): it reads as zero.
+  // Stage the delayed input of the K steps: lanes 0..K-1 of warp 0 each
+  // bulk-copy one slot of this tile (TMA) into shared memory, completing on
+  // one mbarrier that every thread then waits on.  A silenced neuron has no
+  // incoming synapses (sim.py:324-336): its input is masked to zero per step.
   const int sstride = nb * NR;  // elements; < 2**31 / FIS_MAX_BLOCK, checked on the host
   int32_t* rtile = ring + (int64_t)bl * NR + tile * kTile;                 // int32 ring
   uint16_t* rtile16 = reinterpret_cast<uint16_t*>(ring) + (int64_t)bl * NR + tile * kTile;
-  if (kHalf) {
-    // 512 bytes per slot: the first 128 threads copy one word (two neurons)
-    // each; the words land in the first half of sring[k] and are decoded
-    // below, after the copies complete.
-    if (threadIdx.x < kTile / 2) {
-      const uint16_t* src = rtile16 + 2 * threadIdx.x;
-#pragma unroll 4
-      for (int k = 0; k < K; ++k) {
-        cp_async4(&sring[k][threadIdx.x], src);
-        src += sstride;
-      }
+  const unsigned slot_bytes = kHalf ? kTile * 2 : kTile * 4;
+  if (threadIdx.x < kWarp) {
+    if (threadIdx.x == 0) mbar_arrive_expect_tx(&sbar, slot_bytes * (unsigned)K);
+    __syncwarp();
+    if (threadIdx.x < K && !E.inject_stall) {
+      const void* src = kHalf ? (const void*)(rtile16 + (int64_t)threadIdx.x * sstride)
+                              : (const void*)(rtile + (int64_t)threadIdx.x * sstride);
+      bulk_load(&sring[threadIdx.x][0], src, slot_bytes, &sbar);
     }
-    szero[threadIdx.x] = kEmptyPair;
-  } else {
-    const int32_t* src = rtile + threadIdx.x;
-    const bool load = valid && !st.silenced;
-#pragma unroll 4
-    for (int k = 0; k < K; ++k) {
-      if (load) cp_async4(&sring[k][threadIdx.x], src);
-      else sring[k][threadIdx.x] = 0;
-      src += sstride;
-    }
-    szero[threadIdx.x] = 0u;
   }
 
   const int slot0 = ck.slot;  // ring-of-lists slot of step t0
@@ -463,21 +493,32 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
   st.rs = (fl & FIS_FL_NOREFRAC) ? 0.f : E.p.refrac_steps;
   const int64_t own0 = t0 - tr.start;  // the trial's own step at k = 0
 
-  // All staged copies are in shared memory: return the consumed ring slots to
-  // empty with one bulk copy per slot, so the scratch ring needs no clearing
-  // pass and the step loop no stores.
-  cp_async_wait_all();
-  fence_proxy_async_shared();
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    if (kHalf) {
-      for (int k = 0; k < K; ++k) bulk_store(rtile16 + (int64_t)k * sstride, szero, kTile * 2);
-    } else {
-      for (int k = 0; k < K; ++k) bulk_store(rtile + (int64_t)k * sstride, szero, kTile * 4);
+  // Wait for the staged input.  If any thread's wait runs out, the whole CTA
+  // (decided together, so every warp stays whole for its ballots) flags the
+  // error for the host, waits once more for copies still writing its shared
+  // memory, and skips the update, still reaching the final barrier.
+  const unsigned polls = E.wait_polls ? E.wait_polls : kWaitPolls;
+  const bool staged_ok = mbar_wait(&sbar, 0, polls);
+  if (__syncthreads_or(!staged_ok)) {
+    if (threadIdx.x == 0) atomicOr(E.done + 1, (uint32_t)FIS_ERR_STAGE);
+    if (!staged_ok) mbar_wait(&sbar, 0, polls);
+  } else {
+  // The staged slots are in shared memory: warp 0 returns them to empty in
+  // the ring with one bulk store per slot (lanes 0..K-1), so the scratch ring
+  // needs no clearing pass and the step loop no stores.
+  if (threadIdx.x < kWarp) {
+    const uint32_t empty = kHalf ? kEmptyPair : 0u;
+#pragma unroll
+    for (int j = 0; j < kTile / kWarp; ++j) szero[j * kWarp + threadIdx.x] = empty;
+    fence_proxy_async_shared();
+    __syncwarp();
+    if (threadIdx.x < K) {
+      const int k = threadIdx.x;
+      if (kHalf) bulk_store(rtile16 + (int64_t)k * sstride, szero, kTile * 2);
+      else bulk_store(rtile + (int64_t)k * sstride, szero, kTile * 4);
+      bulk_commit();
     }
-    bulk_commit();
   }
-
 
   // Every lane of a warp runs the same loop (the choice depends on the trial
   // and on the warp's ballot only), so every lane reaches each ballot.
@@ -524,14 +565,13 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
     }
   }
 
-  // The barrier above also orders every thread's staged copies before the
-  // loop (with kHalf a thread reads its neighbour's word too).  The drive
-  // precompute runs after it, so warps without driven neurons do not wait
-  // for those that have.
+  // Each thread waited for the staged copies itself (with kHalf it reads its
+  // neighbour's word too).  The drive precompute runs after the wait, so warps
+  // without driven neurons do not wait for those that have.
   Staged in;
   in.col = kHalf ? &sring[0][threadIdx.x >> 1] : &sring[0][threadIdx.x];
   in.shift = (threadIdx.x & 1) * 16;
-  in.mask = (valid && !st.silenced) ? -1 : 0;
+  in.mask = st.silenced ? 0 : -1;
   float nspk;
   if (kTape)
     nspk = step_loop<true, false, kHalf>(st, E, K, ka, kb, valid, 0u, in, sbal[wib], sidx);
@@ -553,15 +593,16 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
   }
   if (spikes_out && valid) spikes_out[sidx] = (st.keep == 0.f) ? 1.f : 0.f;
 
-  // Spike lists and recording for the (rare) steps this neuron fired; the
-  // steps are read back from the staged raster words.
-  if (nspk != 0.f) {
+  // Spike lists and recording for the (rare) steps this neuron fired.
+  uint32_t fired = (uint32_t)nspk;  // bit j is step K-1-j
+  if (fired) {
     const int B = E.batch;
     const bool out_on = !(fl & (FIS_FL_OUT_OFF | FIS_FL_SILENCED));
     const int nch = E.nchunks[i];
     const int slot20 = ck.slot2;
-    for (int k = 0; k < K; ++k) {
-      if (!((sbal[wib][k] >> lane) & 1u)) continue;
+    while (fired) {
+      const int k = K - __ffs(fired);
+      fired &= fired - 1;
       const int sl = slot0 + k < L ? slot0 + k : slot0 + k - L;
       const int sl2 = slot20 + k < 2 * L ? slot20 + k : slot20 + k - 2 * L;
       if ((out_on || k == K - 1) && nch > 0) {
@@ -581,7 +622,8 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
 
   // The clearing copies complete before the CTA ends (szero must stay valid
   // while they read it, and the next scatter adds into these lines).
-  if (threadIdx.x == 0) bulk_wait_all();
+  if (threadIdx.x < K) bulk_wait_all();
+  }  // the staged input arrived
   }  // the trial runs in this block
 
   if (bump) {
@@ -770,7 +812,7 @@ int fis_scatter(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, in
   A.trial_stride = ring_row(e->n);
   A.half = e->ring16 ? 1 : 0;
   const size_t smem = sizeof(int32_t) * (size_t)((k_steps + 1) * nb + 1);
-  k_scatter<<<sm_count() * 4, kScatThreads, smem, (cudaStream_t)stream>>>(*e, A);
+  k_scatter<<<sm_count() * 8, kScatThreads, smem, (cudaStream_t)stream>>>(*e, A);
   return launch_status();
 }
 
@@ -802,13 +844,19 @@ int fis_block(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, int3
   return fis_update(e, b0, nb, k_steps, ring, spikes_out, last_group, stream);
 }
 
-int fis_advance(const fis_engine* e, int64_t steps, int32_t group, int32_t* ring,
+static int record_if(bool on, void* const* events, int64_t idx, cudaStream_t st) {
+  if (!on) return FIS_OK;
+  return (int)cudaEventRecord((cudaEvent_t)events[idx], st);
+}
+
+int fis_advance(const fis_engine* e, int64_t steps, int32_t group, int32_t rows, int32_t* ring,
                 float* spikes_out, void* const* events, int32_t n_pairs, int32_t every,
                 void* stream) {
   int rc = fis_check(e);
   if (rc) return rc;
-  if (steps < 0 || group < 1 || !ring) return FIS_E_ARG;
+  if (steps < 0 || group < 1 || rows < 0 || !ring) return FIS_E_ARG;
   if (events && (n_pairs < 0 || every < 1)) return FIS_E_ARG;
+  const int32_t B = (rows > 0 && rows < e->batch) ? rows : e->batch;
   const int kmax = e->p.lag < FIS_MAX_BLOCK ? e->p.lag : FIS_MAX_BLOCK;
   cudaStream_t st = (cudaStream_t)stream;
   int64_t left = steps;
@@ -816,19 +864,103 @@ int fis_advance(const fis_engine* e, int64_t steps, int32_t group, int32_t* ring
   while (left > 0) {
     const int k = (int)(left < kmax ? left : kmax);
     float* sp = (left == k) ? spikes_out : nullptr;
-    for (int32_t g0 = 0; g0 < e->batch; g0 += group) {
-      const int32_t nb = (e->batch - g0) < group ? (e->batch - g0) : group;
+    for (int32_t g0 = 0; g0 < B; g0 += group) {
+      const int32_t nb = (B - g0) < group ? (B - g0) : group;
       if ((rc = fis_scatter(e, g0, nb, k, ring, stream))) return rc;
       const bool timed = events && (launch % every) == 0 && (launch / every) < n_pairs;
-      if (timed) {
-        if ((rc = (int)cudaEventRecord((cudaEvent_t)events[2 * (launch / every)], st)))
-          return rc;
-      }
-      if ((rc = fis_update(e, g0, nb, k, ring, sp, g0 + nb == e->batch, stream))) return rc;
-      if (timed) {
-        if ((rc = (int)cudaEventRecord((cudaEvent_t)events[2 * (launch / every) + 1], st)))
-          return rc;
-      }
+      if ((rc = record_if(timed, events, 2 * (launch / every), st))) return rc;
+      if ((rc = fis_update(e, g0, nb, k, ring, sp, g0 + nb == B, stream))) return rc;
+      if ((rc = record_if(timed, events, 2 * (launch / every) + 1, st))) return rc;
+      ++launch;
+    }
+    left -= k;
+  }
+  return FIS_OK;
+}
+
+}  // extern "C"
+
+namespace {
+// Per-device side stream and events of fis_advance_overlap, created on first
+// use and kept for the life of the process.
+struct OverlapRes {
+  cudaStream_t side = nullptr;
+  cudaEvent_t after_sc[2] = {nullptr, nullptr};   // scatter of group gi done
+  cudaEvent_t after_upd[2] = {nullptr, nullptr};  // update of group gi done
+  cudaEvent_t block_done = nullptr;               // clock and lists of the block final
+};
+constexpr int kMaxOverlapDevices = 64;
+std::mutex g_overlap_mu;  // held for a whole call: the events are shared
+OverlapRes g_overlap[kMaxOverlapDevices];
+
+int overlap_res(OverlapRes** out) {
+  int dev = 0;
+  cudaError_t err = cudaGetDevice(&dev);
+  if (err != cudaSuccess) return (int)err;
+  if (dev < 0 || dev >= kMaxOverlapDevices) return FIS_E_ARG;
+  OverlapRes& r = g_overlap[dev];
+  if (!r.block_done) {
+    if ((err = cudaStreamCreateWithFlags(&r.side, cudaStreamNonBlocking))) return (int)err;
+    for (int j = 0; j < 2; ++j) {
+      if ((err = cudaEventCreateWithFlags(&r.after_sc[j], cudaEventDisableTiming)))
+        return (int)err;
+      if ((err = cudaEventCreateWithFlags(&r.after_upd[j], cudaEventDisableTiming)))
+        return (int)err;
+    }
+    if ((err = cudaEventCreateWithFlags(&r.block_done, cudaEventDisableTiming))) return (int)err;
+  }
+  *out = &r;
+  return FIS_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int fis_advance_overlap(const fis_engine* e, int64_t steps, int32_t group, int32_t rows,
+                        int32_t* ring2, float* spikes_out, void* const* events,
+                        int32_t n_pairs, int32_t every, void* stream) {
+  int rc = fis_check(e);
+  if (rc) return rc;
+  if (steps < 0 || group < 1 || rows < 0 || !ring2) return FIS_E_ARG;
+  if (events && (n_pairs < 0 || every < 1)) return FIS_E_ARG;
+  const int32_t B = (rows > 0 && rows < e->batch) ? rows : e->batch;
+  const int kmax = e->p.lag < FIS_MAX_BLOCK ? e->p.lag : FIS_MAX_BLOCK;
+  const int32_t gmax = group < B ? group : B;
+  const size_t elem = e->ring16 ? 2 : 4;
+  int32_t* rings[2] = {ring2, reinterpret_cast<int32_t*>(
+                                  reinterpret_cast<char*>(ring2) +
+                                  (size_t)kmax * gmax * ring_row(e->n) * elem)};
+  std::lock_guard<std::mutex> lk(g_overlap_mu);
+  OverlapRes* R = nullptr;
+  if ((rc = overlap_res(&R))) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  // Scatters run on the side stream, updates on the caller's stream; group gi
+  // uses ring gi & 1, so the scatter of group gi + 1 overlaps the update of
+  // group gi.  Scatter gi waits for the update that last drained its ring
+  // (group gi - 2), or for the previous block's last update (gi < 2), which
+  // finalised the clock and the spike lists the scatter reads.
+  if ((rc = (int)cudaEventRecord(R->block_done, st))) return rc;
+  int64_t left = steps;
+  int64_t launch = 0;
+  while (left > 0) {
+    const int k = (int)(left < kmax ? left : kmax);
+    float* sp = (left == k) ? spikes_out : nullptr;
+    int gi = 0;
+    for (int32_t g0 = 0; g0 < B; g0 += group, ++gi) {
+      const int32_t nb = (B - g0) < group ? (B - g0) : group;
+      const bool last = g0 + nb == B;
+      int32_t* ring = rings[gi & 1];
+      cudaEvent_t dep = gi >= 2 ? R->after_upd[gi & 1] : R->block_done;
+      if ((rc = (int)cudaStreamWaitEvent(R->side, dep, 0))) return rc;
+      if ((rc = fis_scatter(e, g0, nb, k, ring, R->side))) return rc;
+      if ((rc = (int)cudaEventRecord(R->after_sc[gi & 1], R->side))) return rc;
+      if ((rc = (int)cudaStreamWaitEvent(st, R->after_sc[gi & 1], 0))) return rc;
+      const bool timed = events && (launch % every) == 0 && (launch / every) < n_pairs;
+      if ((rc = record_if(timed, events, 2 * (launch / every), st))) return rc;
+      if ((rc = fis_update(e, g0, nb, k, ring, sp, last, stream))) return rc;
+      if ((rc = record_if(timed, events, 2 * (launch / every) + 1, st))) return rc;
+      if ((rc = (int)cudaEventRecord(last ? R->block_done : R->after_upd[gi & 1], st)))
+        return rc;
       ++launch;
     }
     left -= k;

@@ -17,7 +17,7 @@ PKG = Path(__file__).resolve().parent
 LIB_NAME = "libfis_b200.so"
 LIB_PATH = PKG / LIB_NAME
 
-FIS_ABI_VERSION = 1
+FIS_ABI_VERSION = 2
 FIS_MAX_BLOCK = 20
 FIS_NOALLOC_RING_INTS = 3 << 20
 REF_EV_ABI = 3
@@ -36,7 +36,7 @@ STATUS = {0: "ok", -1: "FIS_E_ARG (null pointer or size out of range)",
 # Every symbol include/fis.h declares, checked at load time and by the tests.
 EXPORTS = ("ev_spmv_i32", "ev_spmv_i64", "ev_spmv_abi", "fis_abi",
            "fis_sizeof_engine", "fis_sizeof_trial", "fis_check", "fis_block",
-           "fis_scatter", "fis_update", "fis_advance",
+           "fis_scatter", "fis_update", "fis_advance", "fis_advance_overlap",
            "fis_delay_buffer", "fis_spikes_f32", "fis_load_spikes", "fis_add_rows",
            "fis_ring_row", "fis_block_noalloc")
 
@@ -74,6 +74,7 @@ class EngineDesc(ctypes.Structure):
                 ("list_cap", ctypes.c_int64), ("n", ctypes.c_int32),
                 ("batch", ctypes.c_int32), ("chunk", ctypes.c_int32),
                 ("n_recs", ctypes.c_int32), ("ring16", ctypes.c_int32),
+                ("wait_polls", ctypes.c_uint32), ("inject_stall", ctypes.c_uint32),
                 ("pad_", ctypes.c_int32), ("p", LifParams)]
 
 
@@ -104,7 +105,8 @@ def load(path=None):
     L.fis_check.argtypes = [P]
     L.fis_block.argtypes = [P, I32, I32, I32, P, P, I32, P]
     L.fis_scatter.argtypes = [P, I32, I32, I32, P, P]
-    L.fis_advance.argtypes = [P, I64, I32, P, P, P, I32, I32, P]
+    L.fis_advance.argtypes = [P, I64, I32, I32, P, P, P, I32, I32, P]
+    L.fis_advance_overlap.argtypes = [P, I64, I32, I32, P, P, P, I32, I32, P]
     L.fis_update.argtypes = [P, I32, I32, I32, P, P, I32, P]
     L.fis_delay_buffer.argtypes = [P, I32, I32, P, P, P]
     L.fis_spikes_f32.argtypes = [P, I32, I32, I64, P, P]
@@ -117,7 +119,7 @@ def load(path=None):
     L.ev_spmv_i32.argtypes = [P, P, P, P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P]
     L.ev_spmv_i64.argtypes = [P, P, P, P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P]
     for s in ("fis_check", "fis_block", "fis_scatter", "fis_update", "fis_advance",
-              "fis_delay_buffer", "fis_spikes_f32",
+              "fis_advance_overlap", "fis_delay_buffer", "fis_spikes_f32",
               "fis_load_spikes", "fis_add_rows", "ev_spmv_i32", "ev_spmv_i64"):
         getattr(L, s).restype = ctypes.c_int
     if L.fis_abi() != FIS_ABI_VERSION:

@@ -188,21 +188,39 @@ class Batch:
     def run(self, specs, timer=None):
         """Run ``specs`` (at most ``capacity``) to completion; host counts per trial.
 
-        Returns int32 [len(specs)][N] spike counts summed over each trial's
-        bins, copied to the host.
+        Trials are placed longest first, so the running ones always fill the
+        lowest slots: once every trial of the last trial group has ended, that
+        group is no longer launched.  ``slots_of_run[j]`` is the slot that ran
+        ``specs[j]``.  Returns int32 [len(specs)][N] spike counts summed over
+        each trial's bins, in the order of ``specs``, copied to the host.
         """
         c = self.core
-        if len(specs) > self.capacity:
-            raise ValueError("%d trials for %d slots" % (len(specs), self.capacity))
-        slots = list(range(len(specs)))
-        for b in range(len(specs), self.capacity):   # idle slots do nothing
+        k = len(specs)
+        if k > self.capacity:
+            raise ValueError("%d trials for %d slots" % (k, self.capacity))
+        order = sorted(range(k), key=lambda j: -int(specs[j].steps))
+        self.slots_of_run = [0] * k
+        for slot, j in enumerate(order):
+            self.slots_of_run[j] = slot
+        for b in range(k, self.capacity):   # idle slots do nothing
             c.trials[b].start = c.trials[b].end = 0
-        self.load(slots, specs)
-        c.advance(max(int(s.steps) for s in specs), timer=timer)
-        out = self._staging("counts", (len(specs), self.n), torch.int32)
-        dev = torch.stack([self.recording(b).sum(0, dtype=torch.int32) for b in slots])
+        self.load(range(k), [specs[j] for j in order])
+        dur = [int(specs[j].steps) for j in order]
+        G, K = c.group, c.max_block
+        t, total = 0, dur[0] if dur else 0
+        while t < total:
+            active = sum(1 for d in dur if d > t)
+            rows = min(self.capacity, -(-active // G) * G)
+            nxt = dur[(rows - 1) // G * G]   # longest trial of the last group
+            nxt = min(total, t + -(-(nxt - t) // K) * K)  # whole blocks
+            c.advance(nxt - t, timer=timer, rows=rows)
+            t = nxt
+        out = self._staging("counts", (k, self.n), torch.int32)
+        dev = torch.stack([self.recording(self.slots_of_run[j]).sum(0, dtype=torch.int32)
+                           for j in range(k)])
         out.copy_(dev, non_blocking=True)
         torch.cuda.current_stream(c.device).synchronize()
+        c.check_errors()
         return out.numpy().copy()
 
 

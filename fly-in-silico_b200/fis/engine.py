@@ -13,9 +13,10 @@ Layout in HBM (B slots, N neurons, L = lag = buf_len + 1 = 20 by default):
   ``rates`` float32 -- read once and written once per block of up to 20 steps;
 * spike history: ``lists`` uint32 [L][B][cap], ``list_len`` int32 [2L][B],
   ``bits`` uint32 [B][ceil(N/32)][L];
-* scratch ring int32 [K][G][N] for one trial group of G slots, reused by every
-  group: sized to stay resident in the 126 MB L2 between the scatter that fills
-  it and the update that drains it.
+* scratch ring [K][G][NR] (int32, or biased int16 pairs) for one trial group
+  of G slots, reused by every group: sized to stay resident in the 126 MB L2
+  between the scatter that fills it and the update that drains it.  Two such
+  rings when the scatter of one group overlaps the update of the previous one.
 """
 
 from __future__ import annotations
@@ -81,7 +82,8 @@ class Core:
     """B trial slots, their state on the device, and the block launcher."""
 
     def __init__(self, conn: Connectome, batch: int, params=None, device="cuda",
-                 group=None, chunk=None, max_block=_lib.FIS_MAX_BLOCK, ring=None):
+                 group=None, chunk=None, max_block=_lib.FIS_MAX_BLOCK, ring=None,
+                 overlap=True):
         self.device = require_cuda(device)
         self.lib = _lib.load()
         conn.check_bounds()
@@ -91,6 +93,7 @@ class Core:
                 "max |row sum| %.0f >= 2**24: integer accumulation would not be "
                 "exact for this matrix" % ex["max_abs_row_sum"])
         self.conn = conn
+        self.overlap = bool(overlap)
         # Scratch-ring element: biased int16 when no neuron's incoming
         # |count| sum reaches 2**15 (exact, half the ring traffic), else int32.
         ring = ring or os.environ.get("FIS_RING", "auto")
@@ -147,7 +150,8 @@ class Core:
             self.bits = torch.zeros((B, self.words, L), dtype=torch.int32, device=dev)
             # fis_clock: step, then (step mod lag) | (step mod 2*lag) << 32
             self.clock = torch.zeros(2, dtype=torch.int64, device=dev)
-            self.done = torch.zeros(1, dtype=torch.int32, device=dev)
+            # [0] block-completion counter, [1] error bits (FIS_ERR_*)
+            self.done = torch.zeros(2, dtype=torch.int32, device=dev)
         self.trials = (_lib.Trial * B)()
         for b in range(B):
             self.trials[b].start = 0
@@ -185,6 +189,18 @@ class Core:
         d.p = self.P
         _lib.check(self.lib.fis_check(ctypes.byref(d)), "fis_check")
 
+    def check_errors(self):
+        """Raise if a kernel flagged an error since the last check (synchronises).
+
+        A CTA whose staged input did not arrive within its bounded wait skipped
+        its update and set FIS_ERR_STAGE: the state is then not the model's.
+        """
+        err = int(self.done[1].item())
+        if err:
+            self.done[1].zero_()
+            raise RuntimeError("the device reported error bits 0x%x (FIS_ERR_STAGE = 1: "
+                               "a block's staged input did not arrive)" % err)
+
     def set_clock(self, step):
         """Set the device step counter (and its slot indices) and the host mirror."""
         step = int(step)
@@ -201,13 +217,13 @@ class Core:
             group = max(1, RING_L2_BYTES // (self.max_block * self.n * 4))
         self.group = int(max(1, min(int(group), self.batch)))
         self.ring_row = int(self.lib.fis_ring_row(self.n))
+        shape = (2 if self.overlap else 1, self.max_block, self.group, self.ring_row)
         with torch.cuda.device(self.device):
             if self.ring16:   # empty = 0x8000 (biased zero)
-                self.ring = torch.full((self.max_block, self.group, self.ring_row), -32768,
-                                       dtype=torch.int16, device=self.device)
+                self.ring2 = torch.full(shape, -32768, dtype=torch.int16, device=self.device)
             else:
-                self.ring = torch.zeros((self.max_block, self.group, self.ring_row),
-                                        dtype=torch.int32, device=self.device)
+                self.ring2 = torch.zeros(shape, dtype=torch.int32, device=self.device)
+        self.ring = self.ring2[0]
 
     def set_recordings(self, bufs):
         """Recording buffers, each int32 [n_bins][N]; trials point at them by index."""
@@ -301,23 +317,27 @@ class Core:
                                    nb * NR, NR, ctypes.c_void_p(st))
         _lib.check(rc, "fis_add_rows")
 
-    def advance(self, steps, spikes_out=None, timer=None, events=None, every=1):
+    def advance(self, steps, spikes_out=None, timer=None, events=None, every=1, rows=None):
         """``steps`` steps in blocks of at most ``max_block``.
 
-        Runs the native block loop ``fis_advance`` unless restored pending
-        input or a Python ``timer`` needs the per-block path.  ``events``: a
-        list of ``torch.cuda.Event`` pairs (flattened) recorded around every
-        ``every``-th update launch.
+        Runs the native block loop (``fis_advance_overlap`` when there are two
+        or more trial groups and two rings, else ``fis_advance``) unless
+        restored pending input or a Python ``timer`` needs the per-block path.
+        ``events``: a list of ``torch.cuda.Event`` pairs (flattened) recorded
+        around every ``every``-th update launch.  ``rows``: advance only slots
+        [0, rows), as in :meth:`block`.
         """
         steps = int(steps)
         if steps <= 0:
             return
+        nrows = self.batch if rows is None else max(1, min(int(rows), self.batch))
         if self.pending is not None or timer is not None or self.max_block != min(
                 _lib.FIS_MAX_BLOCK, self.lag):
             left = steps
             while left > 0:
                 k = min(left, self.max_block)
-                self.block(k, spikes_out=spikes_out if k == left else None, timer=timer)
+                self.block(k, spikes_out=spikes_out if k == left else None, timer=timer,
+                           rows=nrows)
                 left -= k
             return
         self._sync_trials()
@@ -328,11 +348,14 @@ class Core:
                 e.record(st)
             n_pairs = len(events) // 2
             ev_arr = (ctypes.c_void_p * (2 * n_pairs))(*[e.cuda_event for e in events[:2 * n_pairs]])
-        rc = self.lib.fis_advance(ctypes.byref(self.desc), steps, self.group,
-                                  ctypes.c_void_p(self.ring.data_ptr()),
-                                  ctypes.c_void_p(spikes_out.data_ptr()) if spikes_out is not None else None,
-                                  ev_arr, n_pairs, max(1, int(every)), ctypes.c_void_p(st.cuda_stream))
-        _lib.check(rc, "fis_advance")
+        fn, name = self.lib.fis_advance, "fis_advance"
+        if self.overlap and nrows > self.group:
+            fn, name = self.lib.fis_advance_overlap, "fis_advance_overlap"
+        rc = fn(ctypes.byref(self.desc), steps, self.group, nrows,
+                ctypes.c_void_p(self.ring2.data_ptr()),
+                ctypes.c_void_p(spikes_out.data_ptr()) if spikes_out is not None else None,
+                ev_arr, n_pairs, max(1, int(every)), ctypes.c_void_p(st.cuda_stream))
+        _lib.check(rc, name)
         self.step += steps
 
     def launches_per_block(self):

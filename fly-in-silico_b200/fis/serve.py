@@ -137,6 +137,8 @@ class Server:
 
     def _retire(self):
         done = [rid for rid, (_, _, end, _, _) in self.running.items() if self.core.step >= end]
+        if done:
+            self.core.check_errors()
         for rid in done:
             req, slots, end, rec, t_adm = self.running.pop(rid)
             bins = rec.to(torch.int16).cpu().numpy()

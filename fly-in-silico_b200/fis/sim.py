@@ -763,6 +763,7 @@ def run(stimuli, silenced=None, config: RunConfig | None = None, neurons=None, w
                 break
     torch.cuda.synchronize(c.device)
     t_sim = time.perf_counter() - t1
+    c.check_errors()
     if bar is not None:
         bar.close()
     eng._spikes_version = eng.spikes._version

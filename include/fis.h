@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define FIS_ABI_VERSION 1
+#define FIS_ABI_VERSION 2
 
 /* Largest number of steps one block may advance (registers per thread). */
 #define FIS_MAX_BLOCK 20
@@ -39,6 +39,10 @@ enum {
   FIS_E_BOUNDS = -2,  /* a trial range, block length or slot is out of range */
   FIS_E_ALIGN = -3    /* an array is not 16-byte aligned */
 };
+
+/* Error bits the device sets in done[1].  A CTA whose staged input did not
+ * arrive within wait_polls skipped its update; the run is then invalid. */
+enum { FIS_ERR_STAGE = 1u << 0 };
 
 /* Per-neuron flag bits, one byte per (trial, neuron). */
 enum {
@@ -109,7 +113,9 @@ typedef struct fis_trial {
  *   list_len int32 [2L][B]     entries per (step mod 2L, trial)
  *   bits     uint32 [B][W][L]  spike raster of the last L steps (slot innermost)
  *   clock    fis_clock [1]     global steps completed (device-side)
- *   done     uint32 [1]        block-completion counter, zero between calls
+ *   done     uint32 [2]        [0] block-completion counter, zero between
+ *                              calls; [1] error bits (FIS_ERR_*), set by the
+ *                              device and cleared by the host after reading
  *   recs     int32* [n_recs]   recording buffers [n_bins][N]
  */
 typedef struct fis_engine {
@@ -136,6 +142,10 @@ typedef struct fis_engine {
   int32_t chunk;      /* edges per scatter work item, a multiple of 128     */
   int32_t n_recs;
   int32_t ring16;     /* scratch ring of biased int16 counts (see below)    */
+  uint32_t wait_polls;   /* bound on a CTA's wait for its staged input, in
+                            polls; 0 = the default (~4M, far above any copy) */
+  uint32_t inject_stall; /* test hook: nonzero = issue no staging copy, so
+                            every wait runs out and sets FIS_ERR_STAGE       */
   int32_t pad_;
   fis_lif_params p;
 } fis_engine;
@@ -206,19 +216,37 @@ int fis_update(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps,
                int32_t* ring, float* spikes_out, int32_t last_group, void* stream);
 
 /*
- * Advance every slot by `steps` steps: blocks of min(FIS_MAX_BLOCK, lag)
- * steps (the last one shorter), each block running fis_scatter + fis_update
- * for the trial groups [g0, g0+group) in turn.  The native form of a host
- * loop over fis_block.
- *   ring        int32 [min(FIS_MAX_BLOCK, lag)][group][NR], zero on entry
+ * Advance slots [0, rows) by `steps` steps (rows = 0: every slot): blocks of
+ * min(FIS_MAX_BLOCK, lag) steps (the last one shorter), each block running
+ * fis_scatter + fis_update for the trial groups [g0, g0+group) in turn.  The
+ * native form of a host loop over fis_block.  Slots at or above `rows` must
+ * not be running (their trials ended); they stay frozen.
+ *   ring        [min(FIS_MAX_BLOCK, lag)][group][NR] scratch ring (int32, or
+ *               uint16 pairs when ring16), empty on entry and on return
  *   spikes_out  float [B][N] or NULL, written by the last block
  *   events      NULL, or 2*n_pairs cudaEvent_t handles: pair j is recorded
  *               around the update launch number j*every (0-based over the
  *               whole call), for timing the dominant kernel
  */
-int fis_advance(const fis_engine* e, int64_t steps, int32_t group, int32_t* ring,
-                float* spikes_out, void* const* events, int32_t n_pairs,
-                int32_t every, void* stream);
+int fis_advance(const fis_engine* e, int64_t steps, int32_t group, int32_t rows,
+                int32_t* ring, float* spikes_out, void* const* events,
+                int32_t n_pairs, int32_t every, void* stream);
+
+/*
+ * fis_advance with two scratch rings, so that the scatter of trial group
+ * gi + 1 (on a library-owned side stream, one per device) runs while the
+ * update of group gi runs on `stream`; group gi uses ring gi mod 2.  Ordered
+ * by events: every scatter waits for the update that last drained its ring,
+ * and the first two of a block for the previous block's last update.  On
+ * return all work is ordered before later work on `stream`.
+ *   ring2  two consecutive rings, each min(FIS_MAX_BLOCK, lag) *
+ *          min(group, rows or batch) * NR elements (int32, or uint16 pairs
+ *          when ring16), empty on entry and on return
+ * Other arguments as fis_advance.  Calls are serialised inside the library.
+ */
+int fis_advance_overlap(const fis_engine* e, int64_t steps, int32_t group, int32_t rows,
+                        int32_t* ring2, float* spikes_out, void* const* events,
+                        int32_t n_pairs, int32_t every, void* stream);
 
 /*
  * Write the reference's pending delay ring (Engine.delay_buffer,

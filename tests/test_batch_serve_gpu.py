@@ -53,7 +53,8 @@ def test_batch_trials_match_oracle():
 
     c = conn()
     sp = specs(3, 5, 260)
-    sp[1].steps = 137            # uneven durations: retired in place mid-block
+    sp[0].steps = 61             # uneven durations: retired in place mid-block,
+    sp[1].steps = 137            # and the last trial group dropped once it ends
     sp[2].fire_off = sp[2].stim[:20]
     sp[3].hold, sp[3].v_clamp = np.arange(100, 160), -60.5
     sp[4].out_off, sp[4].in_off = sp[4].stim[20:60], np.arange(500, 700)
@@ -62,10 +63,10 @@ def test_batch_trials_match_oracle():
     for j, s in enumerate(sp):
         o, want = oracle_trial(c, s)
         assert np.array_equal(counts[j], want), j
-        core = b.core
-        assert np.array_equal(core.v[j].cpu().numpy(), o.v[0]), j
-        assert np.array_equal(core.g[j].cpu().numpy(), o.conductance[0]), j
-        assert np.array_equal(core.refrac[j].cpu().numpy(), o.refrac[0]), j
+        core, slot = b.core, b.slots_of_run[j]
+        assert np.array_equal(core.v[slot].cpu().numpy(), o.v[0]), j
+        assert np.array_equal(core.g[slot].cpu().numpy(), o.conductance[0]), j
+        assert np.array_equal(core.refrac[slot].cpu().numpy(), o.refrac[0]), j
 
 
 def test_request_same_alone_and_in_mix():
@@ -105,3 +106,41 @@ def test_server_latency_stats_and_budget():
                    realtime=True)
     st = Server.latency_stats(reps)
     assert st["n"] == 2 and st["p99_s"] >= st["p50_s"] > 0
+
+
+@pytest.mark.parametrize("ring", ["int16", "int32"])
+def test_overlapped_advance_equals_sequential(ring):
+    """Scatter/update overlap on two rings gives the one-ring result, bit for bit."""
+    from fis.batch import Batch
+    from fis.engine import Core
+
+    c = conn()
+    sp = specs(61, 7, (150, 300))   # uneven: trial groups drop out as they end
+    got = []
+    for overlap in (False, True):
+        core = Core(c, 7, group=2, ring=ring, overlap=overlap)
+        counts = Batch(c, 7, core=core).run(sp)
+        got.append((counts, core.v.cpu().numpy(), core.g.cpu().numpy(),
+                    core.refrac.cpu().numpy(), core.step))
+    for a, b in zip(got[0], got[1]):
+        assert np.array_equal(a, b)
+    s = sp[3]
+    assert np.array_equal(got[1][0][3], oracle_trial(c, s)[1])
+
+
+def test_bounded_wait_reports_error_and_context_survives():
+    """A staging wait that runs out sets an error bit the host raises on; the
+    CUDA context stays usable and a fresh batch is exact again."""
+    from fis.batch import Batch
+
+    c = conn()
+    sp = specs(71, 2, 40)
+    b = Batch(c, 2, group=2)
+    b.core.desc.wait_polls = 2000
+    b.core.desc.inject_stall = 1    # no staging copy is issued: every wait runs out
+    with pytest.raises(RuntimeError, match="error bits"):
+        b.run(sp)
+    torch.cuda.synchronize()
+    fresh = Batch(c, 2, group=2).run(sp)
+    for j, s in enumerate(sp):
+        assert np.array_equal(fresh[j], oracle_trial(c, s)[1]), j
