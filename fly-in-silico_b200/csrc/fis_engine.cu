@@ -6,11 +6,14 @@
 //                        conductance exactly at steps t0 .. t0+K-1 (written
 //                        into the reference's ring one step after the spike,
 //                        read buf_len steps later; sim.py:887-897).  Their CSR
-//                        rows are pushed into a scratch ring of K int32 slots
-//                        with integer atomics, a warp per (spike, chunk of
-//                        the row).  Integer sums make the order irrelevant.
+//                        rows are pushed into a scratch ring of K slots of
+//                        integer counts (int32, or two trials' biased int16
+//                        counts per word) with integer atomics, a warp per
+//                        (spike, chunk of the row).  Integer sums make the
+//                        order irrelevant.
 //   phase B  k_update    every neuron of every trial advances K steps with
-//                        its state in registers: refractory counter and gate,
+//                        its state in registers, two trials per thread in
+//                        packed float pairs: refractory counter and gate,
 //                        delayed input, conductance, Poisson drive (Philox),
 //                        membrane, hold, threshold, reset (sim.py:921-952).
 //                        Nothing inside a block depends on a spike of the same
@@ -223,7 +226,10 @@ k_scatter(const fis_engine E, const ScatterArgs A) {
 
   const int lane = threadIdx.x & (kWarp - 1);
   const int warp = threadIdx.x / kWarp;
-  const int64_t slot_stride = (int64_t)A.nb * A.trial_stride;
+  // int32 ring: [slot][trial][trial_stride]; paired int16 ring (half):
+  // [slot][pair][trial_stride] 32-bit words, trial 2p in the low half of each
+  // word and trial 2p + 1 in the high half.
+  const int64_t slot_stride = (int64_t)(A.half ? (A.nb + 1) >> 1 : A.nb) * A.trial_stride;
   for (int32_t w = blockIdx.x * kScatWarps + warp; w < total; w += gridDim.x * kScatWarps) {
     // list holding work item w: largest j with pre_sum[j] <= w
     int lo = 0, hi = nlists - 1;
@@ -257,9 +263,9 @@ k_scatter(const fis_engine E, const ScatterArgs A) {
     if (lo_e >= hi_e) continue;
     // slot_mode 1: (u + 1) mod buf_len = (t0 + kk) mod buf_len, as lag = buf_len + 1
     const int slot = A.slot_mode ? wrap(t_mod_r + kk, E.p.buf_len) : kk;
-    const int64_t row = slot * slot_stride + (int64_t)bl * A.trial_stride;
+    const int64_t row = slot * slot_stride + (int64_t)(A.half ? bl >> 1 : bl) * A.trial_stride;
     int32_t* dst = A.ring + row;
-    uint16_t* dst16 = reinterpret_cast<uint16_t*>(A.ring) + row;
+    const int shift = (bl & 1) * 16;  // the trial's half of a paired word
     // 16-byte vector loads: four edges per lane, 128 edges per warp pass.
     for (int64_t p = (lo_e & ~(int64_t)3) + 4 * lane; p < hi_e; p += 4 * kWarp) {
       const uint4 q = __ldg(reinterpret_cast<const uint4*>(E.edges + p));
@@ -271,10 +277,11 @@ k_scatter(const fis_engine E, const ScatterArgs A) {
           const int post = edge_post(wv[c]);
           if (post < n) {
             if (A.half) {
-              // the pair (post & ~1, post | 1) shares one 32-bit word (rows
-              // are even-sized, so pairs never straddle a row)
-              uint32_t* w = reinterpret_cast<uint32_t*>(dst16 + (post & ~1));
-              atomicAdd(w, (uint32_t)edge_count(wv[c]) << ((post & 1) * 16));
+              // a signed count added to the low half carries into the high
+              // half and back out, leaving it unchanged, while the biased
+              // sums stay inside 0 .. 0xFFFF (exact below 2**15)
+              atomicAdd(reinterpret_cast<uint32_t*>(dst) + post,
+                        (uint32_t)edge_count(wv[c]) << shift);
             } else {
               atomicAdd(dst + post, edge_count(wv[c]));
             }
@@ -286,212 +293,377 @@ k_scatter(const fis_engine E, const ScatterArgs A) {
 }
 
 // ---------------------------------------------------------------------------
-// phase B: K fused steps per neuron
+// phase B: K fused steps per neuron, two trials per thread
 // ---------------------------------------------------------------------------
 
-// One neuron's state for the step loop.
-struct Neuron {
-  float v, g, r;      // membrane, conductance, refractory counter
-  float keep;         // 1 - spike of the previous step
-  float m_fire, m_in, m_hold, v_hold, rs;
-  float v_th;         // threshold; +inf under the fire mask (see lif_step)
-  bool silenced;
+// Packed float pairs.  sm_100 executes add/sub/mul/fma on .f32x2 operands:
+// two independent IEEE binary32 operations per instruction, each lane rounded
+// to nearest even with subnormals kept -- the same bits as two __f*_rn calls,
+// for half the issue slots.  Lane 0 (low word) is trial A of the thread's
+// pair, lane 1 trial B.
+//
+// One caution: the code generator contracts a .f32x2 multiply into the
+// .f32x2 add or subtract that consumes it (one rounding instead of two), even
+// with explicit .rn and with contraction disabled -- measured on B200 with
+// CUDA 12.9, about half of all random operands then differ in the last bit.
+// So a product is never added with add/sub here: addp/subp add it with an FMA
+// by a unit factor known only at run time, p * 1 + c, which is exactly the
+// rounded sum p + c (p * 1 is exact, signed zeros included), and which the
+// code generator cannot fold back into the multiply.
+typedef unsigned long long f2;
+
+__device__ __forceinline__ f2 pk2(float a, float b) {
+  f2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void up2(f2 x, float& a, float& b) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(x));
+}
+__device__ __forceinline__ f2 add2(f2 a, f2 b) {
+  f2 r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f2 sub2(f2 a, f2 b) {
+  f2 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f2 mul2(f2 a, f2 b) {
+  f2 r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
+  f2 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+
+// The state of one neuron in the thread's two trials, and the per-trial
+// constants its flags select.
+struct Pair {
+  f2 v, g, r;        // membrane, conductance, refractory counter
+  f2 keep;           // 1 - spike of the previous step
+  f2 m_in, m_hold, v_hold;
+  float rs0, rs1;    // refractory steps (0 for driven neurons)
+  float vth0, vth1;  // threshold; +inf under the fire mask (see lif_step2)
 };
 
-// One step of sim.py:921-952 for one neuron, the reference's operation order
-// one rounding at a time.  Returns the spike (0 or 1).
-__device__ __forceinline__ float lif_step(Neuron& s, const fis_lif_params& P, int32_t c_in,
-                                          float vstim) {
-  // refractory counter and gate (sim.py:921-923)
-  s.r = __fmul_rn(__fadd_rn(s.r, 1.f), s.keep);
-  const float gate = (s.r >= s.rs) ? 1.f : 0.f;
-  // delayed input and the new conductance (sim.py:928-929); a silenced neuron
-  // has no incoming synapses (sim.py:324-336)
-  const int32_t ck = s.silenced ? 0 : c_in;
-  const float delayed = __fmul_rn(__fmul_rn(P.w_scale, __int2float_rn(ck)), s.m_in);
-  const float gn = __fadd_rn(__fmul_rn(s.g, P.a_syn), __fmul_rn(delayed, gate));
+// The model constants as pairs (both lanes equal).  `one`/`mone` are +-1
+// built from a kernel argument (see addp).
+struct Consts {
+  f2 one, mone, w, a_syn, a_mem, v_rest, v_reset;
+};
+
+// c + p and c - p for a product p, each rounded once as a plain add.
+__device__ __forceinline__ f2 addp(const Consts& C, f2 p, f2 c) { return fma2(p, C.one, c); }
+__device__ __forceinline__ f2 subp(const Consts& C, f2 c, f2 p) { return fma2(p, C.mone, c); }
+
+// One step of sim.py:921-952 for the neuron in both trials, the reference's
+// operation order one rounding at a time.  f0/f1: the spikes; sp: them as
+// floats.
+__device__ __forceinline__ void lif_step2(Pair& s, const Consts& C, float c0, float c1, f2 vstim,
+                                          bool& f0, bool& f1, f2& sp) {
+  // refractory counter and gate (sim.py:921-923); r is the previous step's
+  // product, so its increment is an addp
+  s.r = mul2(addp(C, s.r, C.one), s.keep);
+  float r0, r1;
+  up2(s.r, r0, r1);
+  const f2 gate = pk2(r0 >= s.rs0 ? 1.f : 0.f, r1 >= s.rs1 ? 1.f : 0.f);
+  // delayed input and the new conductance (sim.py:928-929); the counts
+  // arrive already zero for a silenced neuron (no incoming synapses,
+  // sim.py:324-336)
+  const f2 delayed = mul2(mul2(C.w, pk2(c0, c1)), s.m_in);
+  const f2 gn = addp(C, mul2(s.g, C.a_syn), mul2(delayed, gate));
   // membrane with the previous conductance (sim.py:936-938)
-  float v = __fadd_rn(s.v, vstim);
-  v = __fadd_rn(v, __fmul_rn(P.a_mem, __fsub_rn(s.g, __fsub_rn(v, P.v_rest))));
+  f2 v = add2(s.v, vstim);
+  v = addp(C, mul2(C.a_mem, sub2(s.g, sub2(v, C.v_rest))), v);
   // hold, threshold, reset (sim.py:943-952).  spikes = (v > v_th) * m_fire
   // with m_fire in {0, 1} is +0 or 1; comparing against +inf where m_fire is
   // 0 gives the same bits (a finite v never exceeds +inf) without the multiply.
-  v = __fadd_rn(__fmul_rn(v, s.m_hold), s.v_hold);
-  const bool fire = v > s.v_th;
-  const float sp = fire ? 1.f : 0.f;
-  s.v = __fsub_rn(v, __fmul_rn(__fsub_rn(v, P.v_reset), sp));
-  s.g = __fsub_rn(gn, __fmul_rn(gn, sp));
-  s.keep = fire ? 0.f : 1.f;
-  return sp;
+  v = addp(C, mul2(v, s.m_hold), s.v_hold);
+  float v0, v1;
+  up2(v, v0, v1);
+  f0 = v0 > s.vth0;
+  f1 = v1 > s.vth1;
+  sp = pk2(f0 ? 1.f : 0.f, f1 ? 1.f : 0.f);
+  s.v = subp(C, v, mul2(sub2(v, C.v_reset), sp));
+  s.g = subp(C, gn, mul2(gn, sp));
+  s.keep = sub2(C.one, sp);  // 1 - 0 = 1, 1 - 1 = +0: the bits of the select
 }
 
-// The step loop over K steps: `kDrive` selects whether any lane of the warp is
-// driven, so warps without drive carry no drive logic at all.  Returns the
-// number of spikes of this neuron (exact in float).
-// The staged input of step k for this thread: an int32 column, or (kHalf) the
-// thread's half of a biased uint16 pair, masked to zero for silenced neurons
-// and padding lanes.
-struct Staged {
-  const int32_t* col;  // this thread's word of slot 0; slot k is kUpdThreads words further
-  int shift;           // kHalf: 16 for the high half of the pair, else 0
-  int32_t mask;        // kHalf: 0 for a silenced neuron, else all ones
+// The staged input of step k for this thread.  kHalf: one word of the paired
+// ring, trial A's biased count in the low half and trial B's in the high
+// half; flipping each half's top bit turns 0x8000 + c into c as an int16.
+// Otherwise two int32 columns, one per trial.  `mask` zeroes the counts of a
+// silenced neuron, per trial.
+struct Staged2 {
+  const int32_t* col;  // this thread's word of slot 0 (kHalf) or of trial A's row
+  uint32_t mask0, mask1;
+};
+
+// 32-bit words of one staged slot: a pair row (kHalf) or two trial rows
+template <bool kHalf>
+struct StagedRow {
+  static constexpr int kWords = kHalf ? kTile : 2 * kTile;
 };
 
 template <bool kHalf>
-__device__ __forceinline__ int32_t staged(const Staged& s, int k) {
-  const int32_t w = s.col[k * kUpdThreads];
-  if (kHalf) return ((int32_t)(((uint32_t)w >> s.shift) & 0xFFFFu) - 0x8000) & s.mask;
-  return w & s.mask;
+__device__ __forceinline__ void staged2(const Staged2& s, int k, float& c0, float& c1) {
+  if (kHalf) {
+    const uint32_t w = ((uint32_t)s.col[k * kTile] ^ kEmptyPair) & (s.mask0 | s.mask1);
+    c0 = __int2float_rn((int32_t)(int16_t)(w & 0xFFFFu));
+    c1 = __int2float_rn((int32_t)(int16_t)(w >> 16));
+  } else {
+    c0 = __int2float_rn((int32_t)((uint32_t)s.col[k * 2 * kTile] & s.mask0));
+    c1 = __int2float_rn((int32_t)((uint32_t)s.col[k * 2 * kTile + kTile] & s.mask1));
+  }
 }
 
-template <bool kTape, bool kDrive, bool kHalf>
-__device__ __forceinline__ float step_loop(Neuron& st, const fis_engine& E, int K, int ka,
-                                           int kb, bool valid, uint32_t dmask,
-                                           const Staged& in, uint32_t* sbal, int64_t sidx) {
+// The step loop over K steps.  `kDrive` selects whether any lane of the warp
+// is driven in either trial, so warps without drive carry no drive logic.
+// `kPartial`: a trial starts or ends inside this block (or only one of the
+// two runs), so each step commits only the lanes whose trial runs at that
+// step.  Returns the fired steps of each trial as bits, the last step in bit
+// 0 (exact in float).
+template <bool kTape, bool kDrive, bool kHalf, bool kPartial>
+__device__ __forceinline__ f2 step_loop2(Pair& st, const Consts& C, const fis_engine& E, int K,
+                                         int ka0, int kb0, int ka1, int kb1, uint32_t dm0,
+                                         uint32_t dm1, const Staged2& in, uint32_t* sbal0,
+                                         uint32_t* sbal1, int64_t sidx0, int64_t sidx1,
+                                         bool valid) {
   const float kick = E.p.kick;
-  // fired steps as bits, the latest step lowest: m = 2 m + spike per step, an
-  // exact float of at most 20 bits (bookkeeping, not model state, so one fused
-  // multiply-add is fine here)
-  float nspk = 0.f;
-  // Every lane stores the warp's ballot word (the same value to the same
-  // address), so the store needs no lane predicate.
-  if (ka == 0 && kb == K) {
-    // Lanes past the last neuron run the same arithmetic on inert values
-    // (never above an infinite threshold) and store nothing.
-#pragma unroll 4
-    for (int k = 0; k < K; ++k) {
-      const int32_t c_in = staged<kHalf>(in, k);
-      float vstim = 0.f;
-      if (kTape) vstim = valid ? E.vstim[sidx] : 0.f;
-      else if (kDrive) vstim = ((dmask >> k) & 1u) ? kick : 0.f;
-      const float sp = lif_step(st, E.p, c_in, vstim);
-      sbal[k] = __ballot_sync(0xFFFFFFFFu, sp != 0.f);
-      nspk = __fmaf_rn(nspk, 2.f, sp);
+  // fired steps as bits: m = 2 m + spike per step, an exact float of at most
+  // 20 bits (bookkeeping, not model state, so the fused multiply-add is fine)
+  f2 nspk = pk2(0.f, 0.f);
+  const f2 two = pk2(2.f, 2.f);
+  // Lanes past the last neuron run the same arithmetic on inert values (never
+  // above an infinite threshold) and store nothing.  Every lane stores the
+  // warp's ballot word (the same value to the same address), so the store
+  // needs no lane predicate.
+#pragma unroll(kPartial ? 1 : 2)
+  for (int k = 0; k < K; ++k) {
+    float c0, c1;
+    staged2<kHalf>(in, k, c0, c1);
+    f2 vstim = pk2(0.f, 0.f);
+    if (kTape) {
+      vstim = pk2(valid ? E.vstim[sidx0] : 0.f, valid ? E.vstim[sidx1] : 0.f);
+    } else if (kDrive) {
+      vstim = pk2(((dm0 >> k) & 1u) ? kick : 0.f, ((dm1 >> k) & 1u) ? kick : 0.f);
     }
-  } else {
-#pragma unroll 1
-    for (int k = 0; k < K; ++k) {
-      const int32_t c_in = staged<kHalf>(in, k);
-      float sp = 0.f;
-      if (valid && k >= ka && k < kb) {
-        float vstim = 0.f;
-        if (kTape) vstim = E.vstim[sidx];
-        else if (kDrive) vstim = ((dmask >> k) & 1u) ? kick : 0.f;
-        sp = lif_step(st, E.p, c_in, vstim);
-      }
-      sbal[k] = __ballot_sync(0xFFFFFFFFu, sp != 0.f);
-      nspk = __fmaf_rn(nspk, 2.f, sp);
+    bool f0, f1;
+    f2 sp;
+    if (kPartial) {
+      const Pair old = st;
+      lif_step2(st, C, c0, c1, vstim, f0, f1, sp);
+      const bool a0 = k >= ka0 && k < kb0, a1 = k >= ka1 && k < kb1;
+      float x0, x1, y0, y1;
+#define FIS_KEEP_LANES(field)              \
+  up2(st.field, x0, x1);                   \
+  up2(old.field, y0, y1);                  \
+  st.field = pk2(a0 ? x0 : y0, a1 ? x1 : y1);
+      FIS_KEEP_LANES(v)
+      FIS_KEEP_LANES(g)
+      FIS_KEEP_LANES(r)
+      FIS_KEEP_LANES(keep)
+#undef FIS_KEEP_LANES
+      f0 = f0 && a0;
+      f1 = f1 && a1;
+      sp = pk2(f0 ? 1.f : 0.f, f1 ? 1.f : 0.f);
+    } else {
+      lif_step2(st, C, c0, c1, vstim, f0, f1, sp);
     }
+    sbal0[k] = __ballot_sync(0xFFFFFFFFu, f0);
+    sbal1[k] = __ballot_sync(0xFFFFFFFFu, f1);
+    nspk = fma2(nspk, two, sp);
   }
   return nspk;
 }
 
-// Grid: one CTA per (trial of the group, tile of 256 neurons); the trial's
-// rows of the scratch ring are padded to ring_row(n), so each CTA's slice of
-// a ring slot is one aligned 1 KB line of the async bulk copy engine.
+// Grid: one CTA per (pair of trials of the group, tile of 256 neurons).  The
+// scratch ring's rows are padded to ring_row(n), so a tile's slice of a slot
+// is one aligned 1 KB line of the async bulk copy engine: one line per slot
+// of the paired int16 ring, one per trial and slot of the int32 ring.
+// Everything the CTA reads is requested at entry -- the staged input (bulk
+// copies), the clock and trial records, the neuron state -- so their
+// latencies overlap each other and the drive computation.
 template <bool kTape, bool kHalf>
-__global__ void __launch_bounds__(kUpdThreads, 5)
+__global__ void __launch_bounds__(kUpdThreads, 4)
 k_update(const fis_engine E, const int b0, const int nb, const int K,
          int32_t* __restrict__ ring, float* __restrict__ spikes_out,
-         const int bump) {
-  // The block's delayed input, one column per thread: staged here so the step
-  // loop stays rolled (a compact body that fits the instruction cache) and can
-  // index it by step.  With kHalf the staged values are the ring's biased
-  // uint16 pairs, decoded into sring in place.
-  __shared__ __align__(16) int32_t sring[FIS_MAX_BLOCK][kUpdThreads];
-  __shared__ __align__(16) uint32_t szero[kUpdThreads];            // source of the clearing
-  __shared__ uint32_t sdrive[kUpdThreads];                         // kick bit per step
-  __shared__ float sprob[kUpdThreads];                             // Bernoulli p per lane
-  __shared__ uint32_t sbal[kUpdThreads / kWarp][FIS_MAX_BLOCK];    // raster words per step
+         const int bump, const float unit) {  // unit: 1.0f (see addp)
+  // The block's delayed input, a column per thread (per trial for int32):
+  // staged so the step loop stays rolled (a compact body that fits the
+  // instruction cache) and can index it by step.
+  __shared__ __align__(128) int32_t sring[FIS_MAX_BLOCK][StagedRow<kHalf>::kWords];
+  __shared__ __align__(16) uint32_t szero[kTile];                  // source of the clearing
+  __shared__ uint32_t sdrive[2][kUpdThreads];                      // kick bit per step
+  __shared__ float sprob[2][kUpdThreads];                          // p of the j-th driven neuron
+  __shared__ uint16_t sdl[2][kUpdThreads];                         // its thread
+  __shared__ int sndrv[2];                                         // driven neurons counted
+  __shared__ uint32_t sbal[2][kUpdThreads / kWarp][FIS_MAX_BLOCK]; // raster words per step
   __shared__ __align__(8) uint64_t sbar;                           // staging barrier
+  __shared__ fis_clock sck;                                        // the clock, as read
   const int n = E.n;
   const int L = E.p.lag;
   const int Wd = (n + kWarp - 1) / kWarp;
   const int NR = ring_row(n);
-  const int bl = blockIdx.y;    // trial of the group
+  const int pp = blockIdx.y;    // pair of trials of the group: 2 pp, 2 pp + 1
   const int tile = blockIdx.x;  // 256-neuron tile
   const int i = tile * kTile + threadIdx.x;
-  const int b = b0 + bl;
   const int lane = threadIdx.x & (kWarp - 1);
   const int wib = threadIdx.x / kWarp;
   const bool valid = i < n;
   const bool warp_valid = (i - lane) < n;
-  const fis_clock ck = *E.clock;
-  const int64_t t0 = ck.step;
-  const fis_trial tr = E.trials[b];
-  const int ka = (int)max((int64_t)0, min(tr.start - t0, (int64_t)K));
-  const int kb = (int)max((int64_t)0, min(tr.end - t0, (int64_t)K));
-  const int64_t sidx = (int64_t)b * n + i;
+  const int nt = (2 * pp + 1 < nb) ? 2 : 1;  // trials in this pair
+  const int np = (nb + 1) >> 1;              // pairs in the group
+  // slot stride and this tile's offset, in ring elements (uint16 or int32)
+  const int64_t sstride = kHalf ? (int64_t)np * NR * 2 : (int64_t)nb * NR;
+  const int64_t toff = kHalf ? ((int64_t)pp * NR + tile * kTile) * 2
+                             : (int64_t)(2 * pp) * NR + tile * kTile;
+  const int copies = kHalf ? K : K * nt;  // 1 KB lines to stage
 
-  if (ka >= kb) {
-    // The trial does not run in this block (not started, or finished and
-    // frozen in place): only return its ring slots to empty, as scatters of
-    // its last spikes may still land there.  Uniform across the CTA.
-    if (threadIdx.x == 0) {
-      int32_t* rt = ring + (int64_t)bl * NR + tile * kTile;
-      uint16_t* rt16 = reinterpret_cast<uint16_t*>(ring) + (int64_t)bl * NR + tile * kTile;
-      for (int j = threadIdx.x; j < kTile; ++j) szero[j] = kHalf ? kEmptyPair : 0u;
-      fence_proxy_async_shared();
-      const int sst = nb * NR;
-      for (int k = 0; k < K; ++k) {
-        if (kHalf) bulk_store(rt16 + (int64_t)k * sst, szero, kTile * 2);
-        else bulk_store(rt + (int64_t)k * sst, szero, kTile * 4);
-      }
-      bulk_commit();
-      bulk_wait_all();
-    }
-  } else {
-  if (threadIdx.x == 0) {
-    mbar_init(&sbar, 1);
-    fence_mbar_init();
-  }
-  __syncthreads();  // the barrier exists before anyone arrives or waits
-  uint32_t fl = 0;
-  float rate = 0.f;
-  Neuron st;
-  st.v = st.g = st.r = 0.f;
-  if (valid && ka < kb) {
-    st.v = E.v[sidx];
-    st.g = E.g[sidx];
-    st.r = E.refrac[sidx];
-    fl = E.flags[sidx];
-    rate = E.rates[sidx];
-  }
-  st.silenced = fl & FIS_FL_SILENCED;
-
-  // Stage the delayed input of the K steps: lanes 0..K-1 of warp 0 each
-  // bulk-copy one slot of this tile (TMA) into shared memory, completing on
-  // one mbarrier that every thread then waits on.  A silenced neuron has no
-  // incoming synapses (sim.py:324-336): its input is masked to zero per step.
-  const int sstride = nb * NR;  // elements; < 2**31 / FIS_MAX_BLOCK, checked on the host
-  int32_t* rtile = ring + (int64_t)bl * NR + tile * kTile;                 // int32 ring
-  uint16_t* rtile16 = reinterpret_cast<uint16_t*>(ring) + (int64_t)bl * NR + tile * kTile;
-  const unsigned slot_bytes = kHalf ? kTile * 2 : kTile * 4;
+  // Stage the tile's K slots: warp 0 sets up the barrier and issues the bulk
+  // copies (TMA), all completing on that barrier.
   if (threadIdx.x < kWarp) {
-    if (threadIdx.x == 0) mbar_arrive_expect_tx(&sbar, slot_bytes * (unsigned)K);
+    if (threadIdx.x == 0) {
+      mbar_init(&sbar, 1);
+      fence_mbar_init();
+      sndrv[0] = sndrv[1] = 0;
+      mbar_arrive_expect_tx(&sbar, (unsigned)copies * kTile * 4u);
+    }
     __syncwarp();
-    if (threadIdx.x < K && !E.inject_stall) {
-      const void* src = kHalf ? (const void*)(rtile16 + (int64_t)threadIdx.x * sstride)
-                              : (const void*)(rtile + (int64_t)threadIdx.x * sstride);
-      bulk_load(&sring[threadIdx.x][0], src, slot_bytes, &sbar);
+    if (!E.inject_stall) {
+      for (int c = threadIdx.x; c < copies; c += kWarp) {
+        const int k = kHalf ? c : c / nt, t = kHalf ? 0 : c - k * nt;
+        const int64_t off = (int64_t)k * sstride + toff + (int64_t)t * NR;
+        const void* src = kHalf ? (const void*)(reinterpret_cast<const uint16_t*>(ring) + off)
+                                : (const void*)(ring + off);
+        bulk_load(&sring[k][t * kTile], src, kTile * 4u, &sbar);
+      }
     }
   }
 
+  // The clock, read once per CTA by thread 0 and handed to the others in
+  // shared memory.  With `bump` the grid's last CTA advances the clock: every
+  // CTA counts itself in right after its clock read (the count's increment
+  // depends on the value read, so it cannot overtake the read), and the CTA
+  // whose count completes the grid -- by then every CTA has read the clock --
+  // writes the next clock as it ends.  The count's round trip overlaps the
+  // rest of the CTA instead of delaying its exit.
+  unsigned arrived = 0;
+  if (threadIdx.x == 0) {
+    const fis_clock c0 = *E.clock;
+    sck = c0;
+    if (bump) arrived = atomicAdd(E.done, c0.step < 0 ? 2u : 1u) + 1u;  // step >= 0: adds 1
+  }
+  // Per-trial records and state, requested before anything depends on them.
+  fis_trial tr[2];
+  int64_t sidx[2];
+  uint32_t fl[2];
+  float rate[2], vv[2], gg[2], rr[2];
+#pragma unroll
+  for (int t = 0; t < 2; ++t) {
+    const int b = b0 + 2 * pp + (t < nt ? t : 0);
+    tr[t] = E.trials[b];
+    sidx[t] = (int64_t)b * n + i;
+    fl[t] = 0;
+    rate[t] = vv[t] = gg[t] = rr[t] = 0.f;
+    if (valid && t < nt) {
+      vv[t] = E.v[sidx[t]];
+      gg[t] = E.g[sidx[t]];
+      rr[t] = E.refrac[sidx[t]];
+      fl[t] = E.flags[sidx[t]];
+      rate[t] = E.rates[sidx[t]];
+    }
+  }
+  __syncthreads();  // the staging barrier, the drive counters and the clock are set
+  const fis_clock ck = sck;
+  const int64_t t0 = ck.step;
   const int slot0 = ck.slot;  // ring-of-lists slot of step t0
-  // this warp's raster words, one per slot: bits[b][word][slot]
-  uint32_t* bitrow = E.bits + ((int64_t)b * Wd + (i >> 5)) * L;
-  bool s_prev = false;
-  if (warp_valid && t0 - 1 >= tr.start && t0 >= 1)
-    s_prev = (bitrow[slot0 == 0 ? L - 1 : slot0 - 1] >> lane) & 1u;
-  st.keep = s_prev ? 0.f : 1.f;
-  st.m_fire = (!valid || (fl & FIS_FL_FIRE_OFF)) ? 0.f : 1.f;
-  st.v_th = st.m_fire != 0.f ? E.p.v_th : __int_as_float(0x7f800000);
-  st.m_in = (fl & FIS_FL_IN_OFF) ? 0.f : 1.f;
-  const bool hold = fl & FIS_FL_HOLD;
-  st.m_hold = hold ? 0.f : 1.f;
-  st.v_hold = hold ? tr.v_clamp : 0.f;
-  st.rs = (fl & FIS_FL_NOREFRAC) ? 0.f : E.p.refrac_steps;
-  const int64_t own0 = t0 - tr.start;  // the trial's own step at k = 0
+  // A trial slot that does not run in this block is inert: its state is not
+  // used, its threshold infinite, nothing of it stored.
+  int ka[2], kb[2];
+  bool runs[2];
+  uint32_t* bitrow[2];  // this warp's raster words, one per slot: bits[b][word][slot]
+  bool s_prev[2];
+#pragma unroll
+  for (int t = 0; t < 2; ++t) {
+    ka[t] = (int)max((int64_t)0, min(tr[t].start - t0, (int64_t)K));
+    kb[t] = (int)max((int64_t)0, min(tr[t].end - t0, (int64_t)K));
+    runs[t] = t < nt && ka[t] < kb[t];  // uniform across the CTA
+    if (!runs[t]) fl[t] = 0, rate[t] = vv[t] = gg[t] = rr[t] = 0.f;
+    bitrow[t] = E.bits + ((int64_t)(b0 + 2 * pp + (t < nt ? t : 0)) * Wd + (i >> 5)) * L;
+    s_prev[t] = false;
+    if (runs[t] && warp_valid && t0 - 1 >= tr[t].start && t0 >= 1)
+      s_prev[t] = (bitrow[t][slot0 == 0 ? L - 1 : slot0 - 1] >> lane) & 1u;
+  }
+
+  // Poisson drive of the whole block (sim.py:859-861), before the step loop:
+  // draw j of neuron i in a trial is word j % 4 of Philox4x32-10 at counter
+  // (i, j / 4, trial lane) keyed by the trial's seed.  The CTA's driven
+  // neurons are listed per trial in shared memory (in any order: each
+  // contributes only to its own mask) and their (neuron, quad) pairs are
+  // spread over all 256 threads.  It runs while the staged copies fly.
+  uint32_t dm[2] = {0u, 0u};
+  bool warp_driven = false;
+  if (!kTape) {
+    bool drv[2];
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      const float prob = __fmul_rn(rate[t], E.p.prob_scale);
+      drv[t] = valid && runs[t] && prob > 0.f;
+      if (drv[t]) {
+        sdrive[t][threadIdx.x] = 0u;
+        const int pos = atomicAdd(&sndrv[t], 1);
+        sdl[t][pos] = (uint16_t)threadIdx.x;
+        sprob[t][pos] = prob;
+      }
+    }
+    warp_driven = __any_sync(0xFFFFFFFFu, drv[0] || drv[1]);
+    if (__syncthreads_or(drv[0] || drv[1])) {  // also publishes the lists
+      int64_t q0[2];
+      int nq[2], tot[2];
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        const int64_t own0 = t0 - tr[t].start;
+        q0[t] = (own0 + ka[t]) >> 2;
+        nq[t] = runs[t] ? (int)(((own0 + kb[t] - 1) >> 2) - q0[t]) + 1 : 0;
+        tot[t] = sndrv[t] * nq[t];
+      }
+      const uint32_t ibase = (uint32_t)(tile * kTile);
+      for (int itq = threadIdx.x; itq < tot[0] + tot[1]; itq += kUpdThreads) {
+        const int t = itq < tot[0] ? 0 : 1;
+        const int x = itq - (t ? tot[0] : 0);
+        const int nqt = t ? nq[1] : nq[0];
+        const int jd = x / nqt, qq = x - jd * nqt;
+        const int tj = sdl[t][jd];
+        const fis_trial& T = t ? tr[1] : tr[0];
+        const int64_t own0 = t0 - T.start;
+        const int64_t quad = (t ? q0[1] : q0[0]) + qq;
+        const Philox4 r4 = philox4(ibase + (uint32_t)tj, (uint32_t)quad,
+                                   (uint32_t)((uint64_t)quad >> 32), T.stream,
+                                   (uint32_t)T.seed, (uint32_t)(T.seed >> 32));
+        const float pj = sprob[t][jd];
+        const int kq = (int)(quad * 4 - own0);  // step of word 0
+        const int lo = t ? ka[1] : ka[0], hi = t ? kb[1] : kb[0];
+        uint32_t bits = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int k = kq + q;
+          if (k >= lo && k < hi && __fmul_rn((float)(r4.x[q] >> 8), 0x1p-24f) < pj)
+            bits |= 1u << k;
+        }
+        if (bits) atomicOr(&sdrive[t][tj], bits);
+      }
+      __syncthreads();
+#pragma unroll
+      for (int t = 0; t < 2; ++t)
+        if (drv[t]) dm[t] = sdrive[t][threadIdx.x];
+    }
+  }
 
   // Wait for the staged input.  If any thread's wait runs out, the whole CTA
   // (decided together, so every warp stays whole for its ballots) flags the
@@ -503,144 +675,152 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
     if (threadIdx.x == 0) atomicOr(E.done + 1, (uint32_t)FIS_ERR_STAGE);
     if (!staged_ok) mbar_wait(&sbar, 0, polls);
   } else {
-  // The staged slots are in shared memory: warp 0 returns them to empty in
-  // the ring with one bulk store per slot (lanes 0..K-1), so the scratch ring
-  // needs no clearing pass and the step loop no stores.
+  // The staged lines are in shared memory: warp 0 returns them to empty in
+  // the ring with one bulk store each, so the scratch ring needs no clearing
+  // pass and the step loop no stores.  Trials that do not run in this block
+  // are cleared too: scatters of their last spikes may have landed there.
   if (threadIdx.x < kWarp) {
     const uint32_t empty = kHalf ? kEmptyPair : 0u;
 #pragma unroll
     for (int j = 0; j < kTile / kWarp; ++j) szero[j * kWarp + threadIdx.x] = empty;
     fence_proxy_async_shared();
     __syncwarp();
-    if (threadIdx.x < K) {
-      const int k = threadIdx.x;
-      if (kHalf) bulk_store(rtile16 + (int64_t)k * sstride, szero, kTile * 2);
-      else bulk_store(rtile + (int64_t)k * sstride, szero, kTile * 4);
-      bulk_commit();
+    for (int c = threadIdx.x; c < copies; c += kWarp) {
+      const int k = kHalf ? c : c / nt, t = kHalf ? 0 : c - k * nt;
+      const int64_t off = (int64_t)k * sstride + toff + (int64_t)t * NR;
+      if (kHalf) bulk_store(reinterpret_cast<uint16_t*>(ring) + off, szero, kTile * 4u);
+      else bulk_store(ring + off, szero, kTile * 4u);
     }
+    bulk_commit();
   }
 
-  // Every lane of a warp runs the same loop (the choice depends on the trial
-  // and on the warp's ballot only), so every lane reaches each ballot.
-  // Poisson drive of the whole block (sim.py:859-861), before the step loop:
-  // draw j of neuron i is word j % 4 of Philox4x32-10 at counter
-  // (i, j / 4, trial lane); the (neuron, quad) pairs of the warp's driven
-  // neurons are spread over all 32 lanes, and each pair ORs its kick bits into
-  // the neuron's mask.
-  uint32_t dmask = 0;
-  bool warp_driven = false;
-  if (!kTape) {
-    const float prob = __fmul_rn(rate, E.p.prob_scale);
-    const unsigned D = __ballot_sync(0xFFFFFFFFu, valid && ka < kb && prob > 0.f);
-    warp_driven = D != 0u;
-    if (D) {
-      sdrive[threadIdx.x] = 0u;
-      sprob[threadIdx.x] = prob;
-      __syncwarp();
-      const int64_t q0 = (own0 + ka) >> 2;
-      const int nq = (int)(((own0 + kb - 1) >> 2) - q0) + 1;
-      const int total = __popc(D) * nq;
-      const int wbase = threadIdx.x - lane;
-      for (int it = lane; it < total; it += kWarp) {
-        const int jd = it / nq, qq = it - jd * nq;
-        unsigned m = D;
-        for (int t = 0; t < jd; ++t) m &= m - 1;
-        const int j = __ffs(m) - 1;
-        const int64_t quad = q0 + qq;
-        const Philox4 r4 = philox4((uint32_t)(i - lane + j), (uint32_t)quad,
-                                   (uint32_t)((uint64_t)quad >> 32), tr.stream,
-                                   (uint32_t)tr.seed, (uint32_t)(tr.seed >> 32));
-        const float pj = sprob[wbase + j];
-        uint32_t bits = 0;
+  if (runs[0] || runs[1]) {
+  Pair st;
+  float vth[2], rs[2], min_[2], mhold[2], vhold[2];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const int k = (int)(quad * 4 + q - own0);
-          if (k >= ka && k < kb && __fmul_rn((float)(r4.x[q] >> 8), 0x1p-24f) < pj)
-            bits |= 1u << k;
-        }
-        if (bits) atomicOr(&sdrive[wbase + j], bits);
-      }
-      __syncwarp();
-      dmask = sdrive[threadIdx.x];
-    }
+  for (int t = 0; t < 2; ++t) {
+    const bool on = runs[t] && valid && !(fl[t] & FIS_FL_FIRE_OFF);
+    vth[t] = on ? E.p.v_th : __int_as_float(0x7f800000);
+    rs[t] = (fl[t] & FIS_FL_NOREFRAC) ? 0.f : E.p.refrac_steps;
+    min_[t] = (fl[t] & FIS_FL_IN_OFF) ? 0.f : 1.f;
+    const bool hold = fl[t] & FIS_FL_HOLD;
+    mhold[t] = hold ? 0.f : 1.f;
+    vhold[t] = hold ? tr[t].v_clamp : 0.f;
   }
+  st.v = pk2(vv[0], vv[1]);
+  st.g = pk2(gg[0], gg[1]);
+  st.r = pk2(rr[0], rr[1]);
+  st.keep = pk2(s_prev[0] ? 0.f : 1.f, s_prev[1] ? 0.f : 1.f);
+  st.m_in = pk2(min_[0], min_[1]);
+  st.m_hold = pk2(mhold[0], mhold[1]);
+  st.v_hold = pk2(vhold[0], vhold[1]);
+  st.rs0 = rs[0];
+  st.rs1 = rs[1];
+  st.vth0 = vth[0];
+  st.vth1 = vth[1];
+  Consts C;
+  C.one = pk2(unit, unit);
+  C.mone = pk2(-unit, -unit);
+  C.w = pk2(E.p.w_scale, E.p.w_scale);
+  C.a_syn = pk2(E.p.a_syn, E.p.a_syn);
+  C.a_mem = pk2(E.p.a_mem, E.p.a_mem);
+  C.v_rest = pk2(E.p.v_rest, E.p.v_rest);
+  C.v_reset = pk2(E.p.v_reset, E.p.v_reset);
 
-  // Each thread waited for the staged copies itself (with kHalf it reads its
-  // neighbour's word too).  The drive precompute runs after the wait, so warps
-  // without driven neurons do not wait for those that have.
-  Staged in;
-  in.col = kHalf ? &sring[0][threadIdx.x >> 1] : &sring[0][threadIdx.x];
-  in.shift = (threadIdx.x & 1) * 16;
-  in.mask = st.silenced ? 0 : -1;
-  float nspk;
+  // Every lane of a warp runs the same step loop (the choice depends on the
+  // trials and on the warp's vote only), so every lane reaches each ballot.
+  Staged2 in;
+  in.col = &sring[0][threadIdx.x];
+  in.mask0 = (fl[0] & FIS_FL_SILENCED) ? 0u : (kHalf ? 0x0000FFFFu : 0xFFFFFFFFu);
+  in.mask1 = (fl[1] & FIS_FL_SILENCED) ? 0u : (kHalf ? 0xFFFF0000u : 0xFFFFFFFFu);
+  // A trial slot that does not run is inert in the lanes it shares (never
+  // fires, never stored), so only a trial that starts or ends inside the
+  // block needs the per-step commit of the partial loop.
+  const bool full = (!runs[0] || (ka[0] == 0 && kb[0] == K)) &&
+                    (!runs[1] || (ka[1] == 0 && kb[1] == K));
+  uint32_t* sb0 = sbal[0][wib];
+  uint32_t* sb1 = sbal[1][wib];
+  f2 nspk;
   if (kTape)
-    nspk = step_loop<true, false, kHalf>(st, E, K, ka, kb, valid, 0u, in, sbal[wib], sidx);
+    nspk = step_loop2<true, false, kHalf, true>(st, C, E, K, runs[0] ? ka[0] : 0, runs[0] ? kb[0] : 0,
+                                               runs[1] ? ka[1] : 0, runs[1] ? kb[1] : 0, 0u, 0u, in,
+                                               sb0, sb1, sidx[0], sidx[1], valid);
+  else if (!full)
+    nspk = step_loop2<false, true, kHalf, true>(st, C, E, K, runs[0] ? ka[0] : 0,
+                                               runs[0] ? kb[0] : 0, runs[1] ? ka[1] : 0,
+                                               runs[1] ? kb[1] : 0, dm[0], dm[1], in, sb0, sb1,
+                                               sidx[0], sidx[1], valid);
   else if (warp_driven)
-    nspk = step_loop<false, true, kHalf>(st, E, K, ka, kb, valid, dmask, in, sbal[wib], sidx);
+    nspk = step_loop2<false, true, kHalf, false>(st, C, E, K, 0, K, 0, K, dm[0], dm[1], in, sb0,
+                                                sb1, sidx[0], sidx[1], valid);
   else
-    nspk = step_loop<false, false, kHalf>(st, E, K, ka, kb, valid, 0u, in, sbal[wib], sidx);
+    nspk = step_loop2<false, false, kHalf, false>(st, C, E, K, 0, K, 0, K, 0u, 0u, in, sb0, sb1,
+                                                 sidx[0], sidx[1], valid);
   __syncwarp();
-  // the raster words of the K steps into the ring of the last L steps
-  if (lane < K && warp_valid) {
-    const int sl = slot0 + lane < L ? slot0 + lane : slot0 + lane - L;
-    bitrow[sl] = sbal[wib][lane];
-  }
 
-  if (valid && ka < kb) {
-    E.v[sidx] = st.v;
-    E.g[sidx] = st.g;
-    E.refrac[sidx] = st.r;
-  }
-  if (spikes_out && valid) spikes_out[sidx] = (st.keep == 0.f) ? 1.f : 0.f;
-
-  // Spike lists and recording for the (rare) steps this neuron fired.
-  uint32_t fired = (uint32_t)nspk;  // bit j is step K-1-j
-  if (fired) {
-    const int B = E.batch;
-    const bool out_on = !(fl & (FIS_FL_OUT_OFF | FIS_FL_SILENCED));
-    const int nch = E.nchunks[i];
-    const int slot20 = ck.slot2;
-    while (fired) {
-      const int k = K - __ffs(fired);
-      fired &= fired - 1;
-      const int sl = slot0 + k < L ? slot0 + k : slot0 + k - L;
-      const int sl2 = slot20 + k < 2 * L ? slot20 + k : slot20 + k - 2 * L;
-      if ((out_on || k == K - 1) && nch > 0) {
-        const int32_t pos = atomicAdd(E.list_len + (int64_t)sl2 * B + b, nch);
-        uint32_t* dst = E.lists + ((int64_t)sl * B + b) * E.list_cap;
-        for (int q = 0; q < nch; ++q)
-          if (pos + q < E.list_cap) dst[pos + q] = ((uint32_t)i << 8) | (uint32_t)q;
-      }
-      if (tr.rec >= 0 && tr.rec < E.n_recs && tr.bin_steps > 0) {
-        const int64_t own = own0 + k;
-        const int64_t bin = own < 0x7FFFFFFF ? (int64_t)((int)own / tr.bin_steps)
-                                              : own / tr.bin_steps;
-        if (bin < tr.n_bins) atomicAdd(E.recs[tr.rec] + bin * n + i, 1);
+  float ov[2], og[2], orr[2], okeep[2], ospk[2];
+  up2(st.v, ov[0], ov[1]);
+  up2(st.g, og[0], og[1]);
+  up2(st.r, orr[0], orr[1]);
+  up2(st.keep, okeep[0], okeep[1]);
+  up2(nspk, ospk[0], ospk[1]);
+#pragma unroll
+  for (int t = 0; t < 2; ++t) {
+    if (!runs[t]) continue;
+    const int b = b0 + 2 * pp + t;
+    // the raster words of the K steps into the ring of the last L steps
+    if (lane < K && warp_valid) {
+      const int sl = slot0 + lane < L ? slot0 + lane : slot0 + lane - L;
+      bitrow[t][sl] = sbal[t][wib][lane];
+    }
+    if (valid) {
+      E.v[sidx[t]] = ov[t];
+      E.g[sidx[t]] = og[t];
+      E.refrac[sidx[t]] = orr[t];
+      if (spikes_out) spikes_out[sidx[t]] = (okeep[t] == 0.f) ? 1.f : 0.f;
+    }
+    // Spike lists and recording for the (rare) steps this neuron fired.
+    uint32_t fired = (uint32_t)ospk[t];  // bit j is step K-1-j
+    if (fired) {
+      const int B = E.batch;
+      const bool out_on = !(fl[t] & (FIS_FL_OUT_OFF | FIS_FL_SILENCED));
+      const int nch = E.nchunks[i];
+      const int slot20 = ck.slot2;
+      const int64_t own0 = t0 - tr[t].start;
+      while (fired) {
+        const int k = K - __ffs(fired);
+        fired &= fired - 1;
+        const int sl = slot0 + k < L ? slot0 + k : slot0 + k - L;
+        const int sl2 = slot20 + k < 2 * L ? slot20 + k : slot20 + k - 2 * L;
+        if ((out_on || k == K - 1) && nch > 0) {
+          const int32_t pos = atomicAdd(E.list_len + (int64_t)sl2 * B + b, nch);
+          uint32_t* dst = E.lists + ((int64_t)sl * B + b) * E.list_cap;
+          for (int q = 0; q < nch; ++q)
+            if (pos + q < E.list_cap) dst[pos + q] = ((uint32_t)i << 8) | (uint32_t)q;
+        }
+        if (tr[t].rec >= 0 && tr[t].rec < E.n_recs && tr[t].bin_steps > 0) {
+          const int64_t own = own0 + k;
+          const int64_t bin = own < 0x7FFFFFFF ? (int64_t)((int)own / tr[t].bin_steps)
+                                                : own / tr[t].bin_steps;
+          if (bin < tr[t].n_bins) atomicAdd(E.recs[tr[t].rec] + bin * n + i, 1);
+        }
       }
     }
   }
+  }  // a trial of the pair runs in this block
 
   // The clearing copies complete before the CTA ends (szero must stay valid
   // while they read it, and the next scatter adds into these lines).
-  if (threadIdx.x < K) bulk_wait_all();
+  if (threadIdx.x < kWarp) bulk_wait_all();
   }  // the staged input arrived
-  }  // the trial runs in this block
 
-  if (bump) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      __threadfence();
-      const unsigned prev = atomicAdd(E.done, 1u);
-      if (prev == gridDim.x * gridDim.y - 1) {
-        *E.done = 0u;
-        fis_clock next;
-        next.step = t0 + K;
-        next.slot = wrap(ck.slot + K, L);
-        next.slot2 = wrap(ck.slot2 + K, 2 * L);
-        *E.clock = next;
-        __threadfence();
-      }
-    }
+  if (bump && threadIdx.x == 0 && arrived == gridDim.x * gridDim.y) {
+    *E.done = 0u;
+    fis_clock next;
+    next.step = t0 + K;
+    next.slot = wrap(ck.slot + K, L);
+    next.slot2 = wrap(ck.slot2 + K, 2 * L);
+    *E.clock = next;
   }
 }
 
@@ -706,9 +886,10 @@ __global__ void k_load_spikes(const fis_engine E, int b0, int nb,
   }
 }
 
-// dst[r][b][i] += src[r][b][i] with separate row and trial strides; with
-// `half` the destination is the biased uint16 ring (each element is written
-// by one thread only, so a plain 16-bit add is exact).
+// dst[r][b][i] += src[r][b][i] with separate row and trial strides.  With
+// `half` the destination is the paired biased int16 ring: row r, pair b / 2
+// (stride dt words), word i, trial b in half b % 2 -- two threads may share a
+// word, so the add is atomic.
 __global__ void k_add_rows(int n, int nb, int rows, const int32_t* __restrict__ src, int64_t ss,
                            int64_t st, int32_t* __restrict__ dst, int64_t ds, int64_t dt,
                            int half) {
@@ -721,8 +902,8 @@ __global__ void k_add_rows(int n, int nb, int rows, const int32_t* __restrict__ 
     const int64_t r = rb / nb;
     const int32_t v = src[r * ss + bb * st + i];
     if (half) {
-      uint16_t* d = reinterpret_cast<uint16_t*>(dst) + r * ds + bb * dt + i;
-      *d = (uint16_t)(*d + (uint16_t)v);
+      uint32_t* d = reinterpret_cast<uint32_t*>(dst) + r * ds + (bb >> 1) * dt + i;
+      atomicAdd(d, (uint32_t)v << ((bb & 1) * 16));
     } else {
       dst[r * ds + bb * dt + i] += v;
     }
@@ -749,6 +930,12 @@ int grid_for(int64_t total, int threads) {
 }
 
 bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+// 32-bit words of a scratch ring of `k` slots for `nb` trials: [k][nb][NR]
+// int32, or [k][ceil(nb / 2)][NR] words of paired biased int16 counts.
+int64_t ring_words(const fis_engine* e, int k, int nb) {
+  return (int64_t)k * (e->ring16 ? (nb + 1) / 2 : nb) * ring_row(e->n);
+}
 
 int check_range(const fis_engine* e, int32_t b0, int32_t nb) {
   if (b0 < 0 || nb < 1 || (int64_t)b0 + nb > e->batch) return FIS_E_BOUNDS;
@@ -820,19 +1007,19 @@ int fis_update(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, int
                float* spikes_out, int32_t last_group, void* stream) {
   const int rc = check_block(e, b0, nb, k_steps, ring);
   if (rc) return rc;
-  const dim3 ugrid(ring_row(e->n) / kTile, nb);
+  const dim3 ugrid(ring_row(e->n) / kTile, (nb + 1) / 2);  // tiles x trial pairs
   const int bump = last_group ? 1 : 0;
   cudaStream_t st = (cudaStream_t)stream;
   if (e->vstim) {
     if (e->ring16)
-      k_update<true, true><<<ugrid, kUpdThreads, 0, st>>>(*e, b0, nb, k_steps, ring, spikes_out, bump);
+      k_update<true, true><<<ugrid, kUpdThreads, 0, st>>>(*e, b0, nb, k_steps, ring, spikes_out, bump, 1.0f);
     else
-      k_update<true, false><<<ugrid, kUpdThreads, 0, st>>>(*e, b0, nb, k_steps, ring, spikes_out, bump);
+      k_update<true, false><<<ugrid, kUpdThreads, 0, st>>>(*e, b0, nb, k_steps, ring, spikes_out, bump, 1.0f);
   } else {
     if (e->ring16)
-      k_update<false, true><<<ugrid, kUpdThreads, 0, st>>>(*e, b0, nb, k_steps, ring, spikes_out, bump);
+      k_update<false, true><<<ugrid, kUpdThreads, 0, st>>>(*e, b0, nb, k_steps, ring, spikes_out, bump, 1.0f);
     else
-      k_update<false, false><<<ugrid, kUpdThreads, 0, st>>>(*e, b0, nb, k_steps, ring, spikes_out, bump);
+      k_update<false, false><<<ugrid, kUpdThreads, 0, st>>>(*e, b0, nb, k_steps, ring, spikes_out, bump, 1.0f);
   }
   return launch_status();
 }
@@ -926,10 +1113,7 @@ int fis_advance_overlap(const fis_engine* e, int64_t steps, int32_t group, int32
   const int32_t B = (rows > 0 && rows < e->batch) ? rows : e->batch;
   const int kmax = e->p.lag < FIS_MAX_BLOCK ? e->p.lag : FIS_MAX_BLOCK;
   const int32_t gmax = group < B ? group : B;
-  const size_t elem = e->ring16 ? 2 : 4;
-  int32_t* rings[2] = {ring2, reinterpret_cast<int32_t*>(
-                                  reinterpret_cast<char*>(ring2) +
-                                  (size_t)kmax * gmax * ring_row(e->n) * elem)};
+  int32_t* rings[2] = {ring2, ring2 + ring_words(e, kmax, gmax)};
   std::lock_guard<std::mutex> lk(g_overlap_mu);
   OverlapRes* R = nullptr;
   if ((rc = overlap_res(&R))) return rc;
@@ -1026,9 +1210,10 @@ int fis_add_rows(const fis_engine* e, int32_t nb, int32_t rows, const int32_t* s
                  int64_t dst_row_stride, int64_t dst_trial_stride, void* stream) {
   if (!e || !src || !dst || nb < 1 || rows < 0) return FIS_E_ARG;
   if (rows == 0) return FIS_OK;
+  const int32_t drows = e->ring16 ? (nb + 1) >> 1 : nb;  // pairs or trials of dst
   if (src_trial_stride < e->n || dst_trial_stride < e->n ||
       src_row_stride < (int64_t)(nb - 1) * src_trial_stride + e->n ||
-      dst_row_stride < (int64_t)(nb - 1) * dst_trial_stride + e->n)
+      dst_row_stride < (int64_t)(drows - 1) * dst_trial_stride + e->n)
     return FIS_E_BOUNDS;
   const int64_t total = (int64_t)rows * nb * e->n;
   k_add_rows<<<grid_for(total, 256), 256, 0, (cudaStream_t)stream>>>(
@@ -1052,9 +1237,10 @@ int fis_ring_row(int32_t n) { return n < 1 ? FIS_E_ARG : ring_row(n); }
 // from another language and has no device allocator of its own to hand out a
 // buffer.  For them the ring is a fixed array in this library:
 //
-//  * it holds FIS_NOALLOC_RING_INTS int32 (12 MiB): one trial of the
-//    138,639-neuron connectome in 20-step blocks; a call that needs more
-//    (k_steps * nb * fis_ring_row(n) elements) is refused with FIS_E_BOUNDS;
+//  * it holds FIS_NOALLOC_RING_INTS int32 (12 MiB): one trial (or one pair
+//    of trials with the paired int16 ring) of the 138,639-neuron connectome
+//    in 20-step blocks; a call whose ring needs more words is refused with
+//    FIS_E_BOUNDS;
 //  * every GPU that loads this library holds the array until the process
 //    exits;
 //  * all calls on one device share it, so calls that overlap on the GPU (from
@@ -1097,8 +1283,7 @@ extern "C" int fis_block_noalloc(const fis_engine* e, int32_t b0, int32_t nb, in
   int rc = fis_check(e);
   if (rc) return rc;
   if (nb < 1 || k_steps < 1) return FIS_E_BOUNDS;
-  const int64_t elems = (int64_t)k_steps * nb * ring_row(e->n);
-  const int64_t need = e->ring16 ? elems / 2 : elems;  // 32-bit words
+  const int64_t need = ring_words(e, k_steps, nb);
   if (need > (int64_t)FIS_NOALLOC_RING_INTS) return FIS_E_BOUNDS;
   int32_t* ring = nullptr;
   if ((rc = noalloc_ring(&ring))) return rc;

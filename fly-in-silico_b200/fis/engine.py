@@ -211,18 +211,26 @@ class Core:
 
     # --- configuration ---------------------------------------------------
 
+    def ring_rows(self, nb):
+        """Rows of NR 32-bit words per ring slot for ``nb`` trials.
+
+        int32 ring: one row per trial; paired int16 ring: one row per pair of
+        trials (trial 2p in the low half of each word, 2p + 1 in the high).
+        """
+        return (nb + 1) // 2 if self.ring16 else nb
+
     def set_group(self, group=None):
-        """Trial-group size G of the scratch ring [K][G][N] (None: fit in L2)."""
+        """Trial-group size G of the scratch ring (None: fit in L2)."""
         if group is None:
             group = max(1, RING_L2_BYTES // (self.max_block * self.n * 4))
         self.group = int(max(1, min(int(group), self.batch)))
         self.ring_row = int(self.lib.fis_ring_row(self.n))
-        shape = (2 if self.overlap else 1, self.max_block, self.group, self.ring_row)
+        shape = (2 if self.overlap else 1, self.max_block, self.ring_rows(self.group),
+                 self.ring_row)
+        # empty: 0 counts, or the biased zero 0x8000 in both halves of a word
+        empty = -0x7FFF8000 if self.ring16 else 0   # 0x80008000 as int32
         with torch.cuda.device(self.device):
-            if self.ring16:   # empty = 0x8000 (biased zero)
-                self.ring2 = torch.full(shape, -32768, dtype=torch.int16, device=self.device)
-            else:
-                self.ring2 = torch.zeros(shape, dtype=torch.int32, device=self.device)
+            self.ring2 = torch.full(shape, empty, dtype=torch.int32, device=self.device)
         self.ring = self.ring2[0]
 
     def set_recordings(self, bufs):
@@ -309,12 +317,12 @@ class Core:
             return
         n, NR = self.n, self.ring_row
         src = rows[lo - p0, g0]  # [nb][N] starts here; row stride B*N
-        # the kernel's ring for this group is [k][nb][NR]
+        # the kernel's ring for this group: k slots of ring_rows(nb) rows of NR words
+        slot = self.ring_rows(nb) * NR
         rc = self.lib.fis_add_rows(ctypes.byref(self.desc), nb, hi - lo,
                                    ctypes.c_void_p(src.data_ptr()), self.batch * n, n,
-                                   ctypes.c_void_p(self.ring.data_ptr()
-                                                   + (lo - t0) * nb * NR * self.ring.element_size()),
-                                   nb * NR, NR, ctypes.c_void_p(st))
+                                   ctypes.c_void_p(self.ring.data_ptr() + (lo - t0) * slot * 4),
+                                   slot, NR, ctypes.c_void_p(st))
         _lib.check(rc, "fis_add_rows")
 
     def advance(self, steps, spikes_out=None, timer=None, events=None, every=1, rows=None):

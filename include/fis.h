@@ -191,14 +191,18 @@ int fis_check(const fis_engine* e);
  * k_steps steps (refractory gate, delayed input, conductance, Poisson drive,
  * membrane, hold, threshold, reset).  Replaces one call of Engine.step per
  * step (sim.py:745-771, 863-953).
- *   ring        [k_steps][nb][NR], NR = fis_ring_row(N) (N rounded up to a
+ *   ring        the scratch ring, NR = fis_ring_row(N) (N rounded up to a
  *               multiple of 256), 16-byte aligned; "empty" on entry and on
- *               exit.  Elements are int32 counts (empty = 0), or, when
- *               e->ring16 is set, uint16 values 0x8000 + count (empty =
- *               0x8000): exact whenever every neuron's sum of |count| over
- *               its incoming synapses is below 2**15, as then no partial sum
- *               leaves (-2**15, 2**15) and a 32-bit atomic add on a pair of
- *               neighbours never carries across the halves
+ *               exit.  Either int32 counts [k_steps][nb][NR] (empty = 0), or,
+ *               when e->ring16 is set, 32-bit words [k_steps][ceil(nb/2)][NR]
+ *               that pair trials 2p and 2p+1 of the call: uint16 values
+ *               0x8000 + count, trial 2p in the low half (empty word =
+ *               0x80008000).  The pairing is exact whenever every neuron's
+ *               sum of |count| over its incoming synapses is below 2**15, as
+ *               then no partial sum leaves (-2**15, 2**15) and a 32-bit
+ *               atomic add of a sign-extended count into the low half never
+ *               disturbs the high half.  Size in 32-bit words: k_steps *
+ *               (ring16 ? ceil(nb/2) : nb) * NR
  *   spikes_out  float [B][N] or NULL: the spikes of the block's last step
  *   last_group  nonzero when this call completes the block for all trial
  *               groups; the device clock then advances by k_steps
@@ -221,8 +225,8 @@ int fis_update(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps,
  * fis_scatter + fis_update for the trial groups [g0, g0+group) in turn.  The
  * native form of a host loop over fis_block.  Slots at or above `rows` must
  * not be running (their trials ended); they stay frozen.
- *   ring        [min(FIS_MAX_BLOCK, lag)][group][NR] scratch ring (int32, or
- *               uint16 pairs when ring16), empty on entry and on return
+ *   ring        scratch ring of fis_block's layout for min(FIS_MAX_BLOCK,
+ *               lag) slots and `group` trials, empty on entry and on return
  *   spikes_out  float [B][N] or NULL, written by the last block
  *   events      NULL, or 2*n_pairs cudaEvent_t handles: pair j is recorded
  *               around the update launch number j*every (0-based over the
@@ -239,9 +243,9 @@ int fis_advance(const fis_engine* e, int64_t steps, int32_t group, int32_t rows,
  * by events: every scatter waits for the update that last drained its ring,
  * and the first two of a block for the previous block's last update.  On
  * return all work is ordered before later work on `stream`.
- *   ring2  two consecutive rings, each min(FIS_MAX_BLOCK, lag) *
- *          min(group, rows or batch) * NR elements (int32, or uint16 pairs
- *          when ring16), empty on entry and on return
+ *   ring2  two consecutive rings of fis_block's layout, each for
+ *          min(FIS_MAX_BLOCK, lag) slots and min(group, rows or batch)
+ *          trials, empty on entry and on return
  * Other arguments as fis_advance.  Calls are serialised inside the library.
  */
 int fis_advance_overlap(const fis_engine* e, int64_t steps, int32_t group, int32_t rows,
@@ -274,7 +278,9 @@ int fis_load_spikes(const fis_engine* e, int32_t b0, int32_t nb,
 
 /* dst[r][b][i] += src[r][b][i] for r < rows, b < nb, i < N, with row and
  * trial strides given in elements (restore path: pending delayed input that a
- * restored delay ring holds for the next buf_len steps). */
+ * restored delay ring holds for the next buf_len steps).  `dst` is a scratch
+ * ring of fis_block's layout: with e->ring16 its strides count 32-bit words
+ * and step over trial pairs (trial b in half b % 2 of pair b / 2). */
 int fis_add_rows(const fis_engine* e, int32_t nb, int32_t rows,
                  const int32_t* src, int64_t src_row_stride,
                  int64_t src_trial_stride, int32_t* dst, int64_t dst_row_stride,
@@ -288,8 +294,8 @@ int fis_ring_row(int32_t n);
  * of FIS_NOALLOC_RING_INTS int32 (12 MiB) inside this library, for callers
  * that cannot allocate device memory (a real-time closed-loop controller,
  * where an allocation may stall the GPU; a foreign-language host with no
- * device allocator).  No counterpart in the reference.  Larger blocks
- * (k_steps * nb * fis_ring_row(N) > FIS_NOALLOC_RING_INTS) return
+ * device allocator).  No counterpart in the reference.  Blocks whose ring
+ * (fis_block's size in 32-bit words) exceeds FIS_NOALLOC_RING_INTS return
  * FIS_E_BOUNDS.  Every GPU that loads the library keeps the array until
  * exit; calls overlapping on the GPU race on it; each call clears what it
  * uses; the first call on a device looks up the array's address and should

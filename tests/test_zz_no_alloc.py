@@ -73,8 +73,10 @@ def test_noalloc_refuses_blocks_larger_than_its_array(ring, trials):
     conn = C.synthetic()
     lib = L.load()
     nr = lib.fis_ring_row(conn.n)
-    per_trial_words = 20 * nr // (2 if ring == "int16" else 1)
-    assert per_trial_words * (trials - 1) <= L.FIS_NOALLOC_RING_INTS < per_trial_words * trials
+    def words(t):  # ring words of a 20-step block: rows of trials, or of trial pairs
+        return 20 * nr * ((t + 1) // 2 if ring == "int16" else t)
+
+    assert words(trials - 1) <= L.FIS_NOALLOC_RING_INTS < words(trials)
     core = Core(conn, trials, group=trials, ring=ring)
     rc = lib.fis_block_noalloc(ctypes.byref(core.desc), 0, trials, 20, None, 1,
                                ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
