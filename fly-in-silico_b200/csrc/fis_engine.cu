@@ -293,6 +293,89 @@ k_scatter(const fis_engine E, const ScatterArgs A) {
 }
 
 // ---------------------------------------------------------------------------
+// phase A': the block's Poisson drive
+// ---------------------------------------------------------------------------
+
+// Poisson drive of one block (sim.py:859-861) for trials [b0, b0+nb): draw j
+// of neuron i in a trial is word j % 4 of Philox4x32-10 at counter
+// (i, j / 4, trial lane) keyed by the trial's seed, and the neuron is kicked at
+// step j iff float(word >> 8) * 2**-24 < f32(rate) * f32(DT / 1000).  Each warp
+// takes 256 neurons of one trial, lists its driven ones in shared memory and
+// spreads their (neuron, four-step quad) draws over its 32 lanes, so the
+// Philox work is packed whatever the density of driven neurons.  The kick
+// steps of the block go to kicks[b][i] as bits (bit k = step t0 + k), written
+// for neurons with a positive rate only: the update reads them only there.
+constexpr int kDriveThreads = 256;
+constexpr int kDriveSpan = 256;  // neurons per warp task
+
+__global__ void __launch_bounds__(kDriveThreads)
+k_drive(const fis_engine E, const int b0, const int nb, const int K) {
+  __shared__ uint16_t slist[kDriveThreads / kWarp][kDriveSpan];  // offset in the span
+  __shared__ float sprob[kDriveThreads / kWarp][kDriveSpan];
+  __shared__ uint32_t sbits[kDriveThreads / kWarp][kDriveSpan];
+  const int n = E.n;
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int w = threadIdx.x / kWarp;
+  const fis_clock ck = *E.clock;
+  const int64_t t0 = ck.step;
+  const int spans = (n + kDriveSpan - 1) / kDriveSpan;
+  const int64_t tasks = (int64_t)nb * spans;
+  const int64_t nw = (int64_t)gridDim.x * (kDriveThreads / kWarp);
+  for (int64_t task = (int64_t)blockIdx.x * (kDriveThreads / kWarp) + w; task < tasks;
+       task += nw) {
+    const int bl = (int)(task / spans);
+    const int i0 = (int)(task - (int64_t)bl * spans) * kDriveSpan;
+    const int b = b0 + bl;
+    const fis_trial tr = E.trials[b];
+    const int ka = (int)max((int64_t)0, min(tr.start - t0, (int64_t)K));
+    const int kb = (int)max((int64_t)0, min(tr.end - t0, (int64_t)K));
+    if (ka >= kb) continue;  // uniform across the warp
+    const float* rates = E.rates + (int64_t)b * n;
+    int cnt = 0;
+#pragma unroll 4
+    for (int c = 0; c < kDriveSpan / kWarp; ++c) {
+      const int i = i0 + c * kWarp + lane;
+      const float p = i < n ? __fmul_rn(rates[i], E.p.prob_scale) : 0.f;
+      const bool d = p > 0.f;
+      const unsigned m = __ballot_sync(0xFFFFFFFFu, d);
+      if (d) {
+        const int pos = cnt + __popc(m & ((1u << lane) - 1u));
+        slist[w][pos] = (uint16_t)(c * kWarp + lane);
+        sprob[w][pos] = p;
+        sbits[w][pos] = 0u;
+      }
+      cnt += __popc(m);
+    }
+    if (cnt == 0) continue;
+    __syncwarp();
+    const int64_t own0 = t0 - tr.start;  // the trial's own step at k = 0
+    const int64_t q0 = (own0 + ka) >> 2;
+    const int nq = (int)(((own0 + kb - 1) >> 2) - q0) + 1;
+    for (int itq = lane; itq < cnt * nq; itq += kWarp) {
+      const int jd = itq / nq, qq = itq - jd * nq;
+      const int64_t quad = q0 + qq;
+      const Philox4 r4 = philox4((uint32_t)(i0 + slist[w][jd]), (uint32_t)quad,
+                                 (uint32_t)((uint64_t)quad >> 32), tr.stream,
+                                 (uint32_t)tr.seed, (uint32_t)(tr.seed >> 32));
+      const float pj = sprob[w][jd];
+      const int kq = (int)(quad * 4 - own0);  // step of word 0
+      uint32_t bits = 0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int k = kq + q;
+        if (k >= ka && k < kb && __fmul_rn((float)(r4.x[q] >> 8), 0x1p-24f) < pj)
+          bits |= 1u << k;
+      }
+      if (bits) atomicOr(&sbits[w][jd], bits);
+    }
+    __syncwarp();
+    uint32_t* kicks = E.kicks + (int64_t)b * n + i0;
+    for (int j = lane; j < cnt; j += kWarp) kicks[slist[w][j]] = sbits[w][j];
+    __syncwarp();  // the lists are reused by the warp's next task
+  }
+}
+
+// ---------------------------------------------------------------------------
 // phase B: K fused steps per neuron, two trials per thread
 // ---------------------------------------------------------------------------
 
@@ -499,13 +582,8 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
   // instruction cache) and can index it by step.
   __shared__ __align__(128) int32_t sring[FIS_MAX_BLOCK][StagedRow<kHalf>::kWords];
   __shared__ __align__(16) uint32_t szero[kTile];                  // source of the clearing
-  __shared__ uint32_t sdrive[2][kUpdThreads];                      // kick bit per step
-  __shared__ float sprob[2][kUpdThreads];                          // p of the j-th driven neuron
-  __shared__ uint16_t sdl[2][kUpdThreads];                         // its thread
-  __shared__ int sndrv[2];                                         // driven neurons counted
   __shared__ uint32_t sbal[2][kUpdThreads / kWarp][FIS_MAX_BLOCK]; // raster words per step
   __shared__ __align__(8) uint64_t sbar;                           // staging barrier
-  __shared__ fis_clock sck;                                        // the clock, as read
   const int n = E.n;
   const int L = E.p.lag;
   const int Wd = (n + kWarp - 1) / kWarp;
@@ -531,7 +609,6 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
     if (threadIdx.x == 0) {
       mbar_init(&sbar, 1);
       fence_mbar_init();
-      sndrv[0] = sndrv[1] = 0;
       mbar_arrive_expect_tx(&sbar, (unsigned)copies * kTile * 4u);
     }
     __syncwarp();
@@ -546,30 +623,20 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
     }
   }
 
-  // The clock, read once per CTA by thread 0 and handed to the others in
-  // shared memory.  With `bump` the grid's last CTA advances the clock: every
-  // CTA counts itself in right after its clock read (the count's increment
-  // depends on the value read, so it cannot overtake the read), and the CTA
-  // whose count completes the grid -- by then every CTA has read the clock --
-  // writes the next clock as it ends.  The count's round trip overlaps the
-  // rest of the CTA instead of delaying its exit.
-  unsigned arrived = 0;
-  if (threadIdx.x == 0) {
-    const fis_clock c0 = *E.clock;
-    sck = c0;
-    if (bump) arrived = atomicAdd(E.done, c0.step < 0 ? 2u : 1u) + 1u;  // step >= 0: adds 1
-  }
-  // Per-trial records and state, requested before anything depends on them.
+  // Clock, trial records and state, requested before anything depends on
+  // them.  A trial slot that does not run in this block is inert: its state
+  // is not used, its threshold infinite, nothing of it stored.
+  const fis_clock ck = *E.clock;
   fis_trial tr[2];
   int64_t sidx[2];
-  uint32_t fl[2];
+  uint32_t fl[2], dm[2];
   float rate[2], vv[2], gg[2], rr[2];
 #pragma unroll
   for (int t = 0; t < 2; ++t) {
     const int b = b0 + 2 * pp + (t < nt ? t : 0);
     tr[t] = E.trials[b];
     sidx[t] = (int64_t)b * n + i;
-    fl[t] = 0;
+    fl[t] = dm[t] = 0;
     rate[t] = vv[t] = gg[t] = rr[t] = 0.f;
     if (valid && t < nt) {
       vv[t] = E.v[sidx[t]];
@@ -577,93 +644,32 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
       rr[t] = E.refrac[sidx[t]];
       fl[t] = E.flags[sidx[t]];
       rate[t] = E.rates[sidx[t]];
+      if (!kTape) dm[t] = E.kicks[sidx[t]];
     }
   }
-  __syncthreads();  // the staging barrier, the drive counters and the clock are set
-  const fis_clock ck = sck;
+  __syncthreads();  // the staging barrier exists before anyone waits on it
   const int64_t t0 = ck.step;
   const int slot0 = ck.slot;  // ring-of-lists slot of step t0
-  // A trial slot that does not run in this block is inert: its state is not
-  // used, its threshold infinite, nothing of it stored.
   int ka[2], kb[2];
   bool runs[2];
   uint32_t* bitrow[2];  // this warp's raster words, one per slot: bits[b][word][slot]
   bool s_prev[2];
+  bool drv_any = false;
 #pragma unroll
   for (int t = 0; t < 2; ++t) {
     ka[t] = (int)max((int64_t)0, min(tr[t].start - t0, (int64_t)K));
     kb[t] = (int)max((int64_t)0, min(tr[t].end - t0, (int64_t)K));
     runs[t] = t < nt && ka[t] < kb[t];  // uniform across the CTA
     if (!runs[t]) fl[t] = 0, rate[t] = vv[t] = gg[t] = rr[t] = 0.f;
+    // kick steps were computed by phase A for neurons with a positive rate
+    if (!(runs[t] && __fmul_rn(rate[t], E.p.prob_scale) > 0.f)) dm[t] = 0u;
+    drv_any = drv_any || (valid && runs[t] && __fmul_rn(rate[t], E.p.prob_scale) > 0.f);
     bitrow[t] = E.bits + ((int64_t)(b0 + 2 * pp + (t < nt ? t : 0)) * Wd + (i >> 5)) * L;
     s_prev[t] = false;
     if (runs[t] && warp_valid && t0 - 1 >= tr[t].start && t0 >= 1)
       s_prev[t] = (bitrow[t][slot0 == 0 ? L - 1 : slot0 - 1] >> lane) & 1u;
   }
-
-  // Poisson drive of the whole block (sim.py:859-861), before the step loop:
-  // draw j of neuron i in a trial is word j % 4 of Philox4x32-10 at counter
-  // (i, j / 4, trial lane) keyed by the trial's seed.  The CTA's driven
-  // neurons are listed per trial in shared memory (in any order: each
-  // contributes only to its own mask) and their (neuron, quad) pairs are
-  // spread over all 256 threads.  It runs while the staged copies fly.
-  uint32_t dm[2] = {0u, 0u};
-  bool warp_driven = false;
-  if (!kTape) {
-    bool drv[2];
-#pragma unroll
-    for (int t = 0; t < 2; ++t) {
-      const float prob = __fmul_rn(rate[t], E.p.prob_scale);
-      drv[t] = valid && runs[t] && prob > 0.f;
-      if (drv[t]) {
-        sdrive[t][threadIdx.x] = 0u;
-        const int pos = atomicAdd(&sndrv[t], 1);
-        sdl[t][pos] = (uint16_t)threadIdx.x;
-        sprob[t][pos] = prob;
-      }
-    }
-    warp_driven = __any_sync(0xFFFFFFFFu, drv[0] || drv[1]);
-    if (__syncthreads_or(drv[0] || drv[1])) {  // also publishes the lists
-      int64_t q0[2];
-      int nq[2], tot[2];
-#pragma unroll
-      for (int t = 0; t < 2; ++t) {
-        const int64_t own0 = t0 - tr[t].start;
-        q0[t] = (own0 + ka[t]) >> 2;
-        nq[t] = runs[t] ? (int)(((own0 + kb[t] - 1) >> 2) - q0[t]) + 1 : 0;
-        tot[t] = sndrv[t] * nq[t];
-      }
-      const uint32_t ibase = (uint32_t)(tile * kTile);
-      for (int itq = threadIdx.x; itq < tot[0] + tot[1]; itq += kUpdThreads) {
-        const int t = itq < tot[0] ? 0 : 1;
-        const int x = itq - (t ? tot[0] : 0);
-        const int nqt = t ? nq[1] : nq[0];
-        const int jd = x / nqt, qq = x - jd * nqt;
-        const int tj = sdl[t][jd];
-        const fis_trial& T = t ? tr[1] : tr[0];
-        const int64_t own0 = t0 - T.start;
-        const int64_t quad = (t ? q0[1] : q0[0]) + qq;
-        const Philox4 r4 = philox4(ibase + (uint32_t)tj, (uint32_t)quad,
-                                   (uint32_t)((uint64_t)quad >> 32), T.stream,
-                                   (uint32_t)T.seed, (uint32_t)(T.seed >> 32));
-        const float pj = sprob[t][jd];
-        const int kq = (int)(quad * 4 - own0);  // step of word 0
-        const int lo = t ? ka[1] : ka[0], hi = t ? kb[1] : kb[0];
-        uint32_t bits = 0;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const int k = kq + q;
-          if (k >= lo && k < hi && __fmul_rn((float)(r4.x[q] >> 8), 0x1p-24f) < pj)
-            bits |= 1u << k;
-        }
-        if (bits) atomicOr(&sdrive[t][tj], bits);
-      }
-      __syncthreads();
-#pragma unroll
-      for (int t = 0; t < 2; ++t)
-        if (drv[t]) dm[t] = sdrive[t][threadIdx.x];
-    }
-  }
+  const bool warp_driven = !kTape && __any_sync(0xFFFFFFFFu, drv_any);
 
   // Wait for the staged input.  If any thread's wait runs out, the whole CTA
   // (decided together, so every warp stays whole for its ballots) flags the
@@ -671,7 +677,15 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
   // memory, and skips the update, still reaching the final barrier.
   const unsigned polls = E.wait_polls ? E.wait_polls : kWaitPolls;
   const bool staged_ok = mbar_wait(&sbar, 0, polls);
-  if (__syncthreads_or(!staged_ok)) {
+  const bool failed = __syncthreads_or(!staged_ok);
+  // With `bump` the grid's last CTA advances the clock.  Each CTA counts
+  // itself in here, after a barrier that every one of its threads reached
+  // with the clock already read, and the CTA whose count completes the grid
+  // -- by then every CTA has read the clock -- writes the next clock as it
+  // ends; the count's round trip overlaps the rest of the CTA.
+  unsigned arrived = 0;
+  if (bump && threadIdx.x == 0) arrived = atomicAdd(E.done, 1u) + 1u;
+  if (failed) {
     if (threadIdx.x == 0) atomicOr(E.done + 1, (uint32_t)FIS_ERR_STAGE);
     if (!staged_ok) mbar_wait(&sbar, 0, polls);
   } else {
@@ -957,7 +971,7 @@ int fis_check(const fis_engine* e) {
   if (!e) return FIS_E_ARG;
   if (!e->row_ptr || !e->edges || !e->nchunks || !e->v || !e->g || !e->refrac ||
       !e->flags || !e->rates || !e->trials || !e->lists || !e->list_len ||
-      !e->bits || !e->clock || !e->done)
+      !e->bits || !e->clock || !e->done || !e->kicks)
     return FIS_E_ARG;
   if (e->n < 1 || e->n > (1 << 18) || e->batch < 1 || e->nnz < 0) return FIS_E_ARG;
   if (e->chunk < 128 || (e->chunk % 128) != 0) return FIS_E_ARG;
@@ -1000,6 +1014,13 @@ int fis_scatter(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, in
   A.half = e->ring16 ? 1 : 0;
   const size_t smem = sizeof(int32_t) * (size_t)((k_steps + 1) * nb + 1);
   k_scatter<<<sm_count() * 8, kScatThreads, smem, (cudaStream_t)stream>>>(*e, A);
+  int rc2 = launch_status();
+  if (rc2 || e->vstim) return rc2;  // an external drive replaces the Philox draw
+  const int64_t warps = (int64_t)nb * ((e->n + kDriveSpan - 1) / kDriveSpan);
+  const int64_t cap = (int64_t)sm_count() * 8;
+  const int64_t blocks = (warps + kDriveThreads / kWarp - 1) / (kDriveThreads / kWarp);
+  k_drive<<<(int)(blocks < cap ? blocks : cap), kDriveThreads, 0, (cudaStream_t)stream>>>(
+      *e, b0, nb, k_steps);
   return launch_status();
 }
 

@@ -17,7 +17,7 @@ PKG = Path(__file__).resolve().parent
 LIB_NAME = "libfis_b200.so"
 LIB_PATH = PKG / LIB_NAME
 
-FIS_ABI_VERSION = 2
+FIS_ABI_VERSION = 3
 FIS_MAX_BLOCK = 20
 FIS_NOALLOC_RING_INTS = 3 << 20
 REF_EV_ABI = 3
@@ -70,7 +70,8 @@ class EngineDesc(ctypes.Structure):
                 ("vstim", ctypes.c_void_p), ("trials", ctypes.c_void_p), ("lists", ctypes.c_void_p),
                 ("list_len", ctypes.c_void_p), ("bits", ctypes.c_void_p),
                 ("clock", ctypes.c_void_p), ("done", ctypes.c_void_p),
-                ("recs", ctypes.c_void_p), ("nnz", ctypes.c_int64),
+                ("recs", ctypes.c_void_p), ("kicks", ctypes.c_void_p),
+                ("nnz", ctypes.c_int64),
                 ("list_cap", ctypes.c_int64), ("n", ctypes.c_int32),
                 ("batch", ctypes.c_int32), ("chunk", ctypes.c_int32),
                 ("n_recs", ctypes.c_int32), ("ring16", ctypes.c_int32),

@@ -152,6 +152,8 @@ class Core:
             self.clock = torch.zeros(2, dtype=torch.int64, device=dev)
             # [0] block-completion counter, [1] error bits (FIS_ERR_*)
             self.done = torch.zeros(2, dtype=torch.int32, device=dev)
+            # kick steps of the current block per driven (trial, neuron)
+            self.kicks = torch.zeros((B, n), dtype=torch.int32, device=dev)
         self.trials = (_lib.Trial * B)()
         for b in range(B):
             self.trials[b].start = 0
@@ -181,6 +183,7 @@ class Core:
         d.bits = self.bits.data_ptr()
         d.clock = self.clock.data_ptr()
         d.done = self.done.data_ptr()
+        d.kicks = self.kicks.data_ptr()
         d.recs = None
         d.nnz = nnz
         d.list_cap = self.list_cap

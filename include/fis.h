@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define FIS_ABI_VERSION 2
+#define FIS_ABI_VERSION 3
 
 /* Largest number of steps one block may advance (registers per thread). */
 #define FIS_MAX_BLOCK 20
@@ -117,6 +117,9 @@ typedef struct fis_trial {
  *                              calls; [1] error bits (FIS_ERR_*), set by the
  *                              device and cleared by the host after reading
  *   recs     int32* [n_recs]   recording buffers [n_bins][N]
+ *   kicks    uint32 [B][N]     scratch: the Poisson kick steps of the current
+ *                              block, written by phase A for neurons with a
+ *                              positive rate (others are never read)
  */
 typedef struct fis_engine {
   const int64_t* row_ptr;
@@ -135,6 +138,7 @@ typedef struct fis_engine {
   fis_clock* clock;
   uint32_t* done;
   int32_t* const* recs;
+  uint32_t* kicks;
   int64_t nnz;
   int64_t list_cap;
   int32_t n;
@@ -211,7 +215,8 @@ int fis_block(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps,
               int32_t* ring, float* spikes_out, int32_t last_group,
               void* stream);
 
-/* Phase A of fis_block alone: the scatter into `ring` (same arguments). */
+/* Phase A of fis_block alone: the scatter into `ring` and the block's Poisson
+ * drive into e->kicks (same arguments). */
 int fis_scatter(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps,
                 int32_t* ring, void* stream);
 
