@@ -155,6 +155,8 @@ struct ScatterArgs {
   int32_t* ring;      // slot stride nb*trial_stride elements
   int trial_stride;   // elements per trial row of `ring`
   int half;           // elements are biased uint16 (see fis.h), else int32
+  fis_clock clk;      // the block's clock when clk_given, else *E.clock
+  int clk_given;
 };
 
 // The value that marks an empty pair of biased uint16 ring elements.
@@ -166,7 +168,7 @@ k_scatter(const fis_engine E, const ScatterArgs A) {
   const int n = E.n;
   const int B = E.batch;
   const int L = E.p.lag;
-  const fis_clock ck = *E.clock;
+  const fis_clock ck = A.clk_given ? A.clk : *E.clock;
   const int64_t t0 = ck.step;
   const int64_t u_first = t0 + A.u_off;  // u_off is -lag: u_first = t0 mod lag
   const int64_t u_last = t0 - 1;
@@ -309,14 +311,15 @@ constexpr int kDriveThreads = 256;
 constexpr int kDriveSpan = 256;  // neurons per warp task
 
 __global__ void __launch_bounds__(kDriveThreads)
-k_drive(const fis_engine E, const int b0, const int nb, const int K) {
+k_drive(const fis_engine E, const int b0, const int nb, const int K, const fis_clock clk,
+        const int clk_given) {
   __shared__ uint16_t slist[kDriveThreads / kWarp][kDriveSpan];  // offset in the span
   __shared__ float sprob[kDriveThreads / kWarp][kDriveSpan];
   __shared__ uint32_t sbits[kDriveThreads / kWarp][kDriveSpan];
   const int n = E.n;
   const int lane = threadIdx.x & (kWarp - 1);
   const int w = threadIdx.x / kWarp;
-  const fis_clock ck = *E.clock;
+  const fis_clock ck = clk_given ? clk : *E.clock;
   const int64_t t0 = ck.step;
   const int spans = (n + kDriveSpan - 1) / kDriveSpan;
   const int64_t tasks = (int64_t)nb * spans;
@@ -576,7 +579,8 @@ template <bool kTape, bool kHalf>
 __global__ void __launch_bounds__(kUpdThreads, 4)
 k_update(const fis_engine E, const int b0, const int nb, const int K,
          int32_t* __restrict__ ring, float* __restrict__ spikes_out,
-         const int bump, const float unit) {  // unit: 1.0f (see addp)
+         const int bump, const float unit,  // unit: 1.0f (see addp)
+         const fis_clock clk, const int clk_given) {
   // The block's delayed input, a column per thread (per trial for int32):
   // staged so the step loop stays rolled (a compact body that fits the
   // instruction cache) and can index it by step.
@@ -626,7 +630,7 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
   // Clock, trial records and state, requested before anything depends on
   // them.  A trial slot that does not run in this block is inert: its state
   // is not used, its threshold infinite, nothing of it stored.
-  const fis_clock ck = *E.clock;
+  const fis_clock ck = clk_given ? clk : *E.clock;  // the block's clock
   fis_trial tr[2];
   int64_t sidx[2];
   uint32_t fl[2], dm[2];
@@ -997,8 +1001,23 @@ static int check_block(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_st
   return FIS_OK;
 }
 
-int fis_scatter(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, int32_t* ring,
-                void* stream) {
+}  // extern "C"
+
+namespace {
+
+// The block's clock for a launch inside fis_advance*: the host knows every
+// block's step there, so launches need not wait for the device clock to be
+// advanced between blocks (only the call's last launch advances it).
+fis_clock clock_at(const fis_engine* e, int64_t step) {
+  fis_clock c;
+  c.step = step;
+  c.slot = (int32_t)(step % e->p.lag);
+  c.slot2 = (int32_t)(step % (2 * e->p.lag));
+  return c;
+}
+
+int scatter_block(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, int32_t* ring,
+                  cudaStream_t st, const fis_clock* clk) {
   const int rc = check_block(e, b0, nb, k_steps, ring);
   if (rc) return rc;
   ScatterArgs A;
@@ -1012,90 +1031,68 @@ int fis_scatter(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, in
   A.ring = ring;
   A.trial_stride = ring_row(e->n);
   A.half = e->ring16 ? 1 : 0;
+  A.clk_given = clk ? 1 : 0;
+  if (clk) A.clk = *clk;
   const size_t smem = sizeof(int32_t) * (size_t)((k_steps + 1) * nb + 1);
-  k_scatter<<<sm_count() * 8, kScatThreads, smem, (cudaStream_t)stream>>>(*e, A);
+  k_scatter<<<sm_count() * 8, kScatThreads, smem, st>>>(*e, A);
   int rc2 = launch_status();
   if (rc2 || e->vstim) return rc2;  // an external drive replaces the Philox draw
   const int64_t warps = (int64_t)nb * ((e->n + kDriveSpan - 1) / kDriveSpan);
   const int64_t cap = (int64_t)sm_count() * 8;
   const int64_t blocks = (warps + kDriveThreads / kWarp - 1) / (kDriveThreads / kWarp);
-  k_drive<<<(int)(blocks < cap ? blocks : cap), kDriveThreads, 0, (cudaStream_t)stream>>>(
-      *e, b0, nb, k_steps);
+  k_drive<<<(int)(blocks < cap ? blocks : cap), kDriveThreads, 0, st>>>(
+      *e, b0, nb, k_steps, A.clk, A.clk_given);
   return launch_status();
 }
 
-int fis_update(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, int32_t* ring,
-               float* spikes_out, int32_t last_group, void* stream) {
+int update_block(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, int32_t* ring,
+                 float* spikes_out, int32_t bump, cudaStream_t st, const fis_clock* clk) {
   const int rc = check_block(e, b0, nb, k_steps, ring);
   if (rc) return rc;
   const dim3 ugrid(ring_row(e->n) / kTile, (nb + 1) / 2);  // tiles x trial pairs
-  const int bump = last_group ? 1 : 0;
-  cudaStream_t st = (cudaStream_t)stream;
+  fis_clock c{};
+  if (clk) c = *clk;
+  const int given = clk ? 1 : 0;
+  const int bp = bump ? 1 : 0;
   if (e->vstim) {
     if (e->ring16)
-      k_update<true, true><<<ugrid, kUpdThreads, 0, st>>>(*e, b0, nb, k_steps, ring, spikes_out, bump, 1.0f);
+      k_update<true, true><<<ugrid, kUpdThreads, 0, st>>>(*e, b0, nb, k_steps, ring, spikes_out,
+                                                          bp, 1.0f, c, given);
     else
-      k_update<true, false><<<ugrid, kUpdThreads, 0, st>>>(*e, b0, nb, k_steps, ring, spikes_out, bump, 1.0f);
+      k_update<true, false><<<ugrid, kUpdThreads, 0, st>>>(*e, b0, nb, k_steps, ring, spikes_out,
+                                                           bp, 1.0f, c, given);
   } else {
     if (e->ring16)
-      k_update<false, true><<<ugrid, kUpdThreads, 0, st>>>(*e, b0, nb, k_steps, ring, spikes_out, bump, 1.0f);
+      k_update<false, true><<<ugrid, kUpdThreads, 0, st>>>(*e, b0, nb, k_steps, ring, spikes_out,
+                                                           bp, 1.0f, c, given);
     else
-      k_update<false, false><<<ugrid, kUpdThreads, 0, st>>>(*e, b0, nb, k_steps, ring, spikes_out, bump, 1.0f);
+      k_update<false, false><<<ugrid, kUpdThreads, 0, st>>>(*e, b0, nb, k_steps, ring,
+                                                            spikes_out, bp, 1.0f, c, given);
   }
   return launch_status();
 }
 
-int fis_block(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, int32_t* ring,
-              float* spikes_out, int32_t last_group, void* stream) {
-  const int rc = fis_scatter(e, b0, nb, k_steps, ring, stream);
-  if (rc) return rc;
-  return fis_update(e, b0, nb, k_steps, ring, spikes_out, last_group, stream);
-}
-
-static int record_if(bool on, void* const* events, int64_t idx, cudaStream_t st) {
+int record_if(bool on, void* const* events, int64_t idx, cudaStream_t st) {
   if (!on) return FIS_OK;
   return (int)cudaEventRecord((cudaEvent_t)events[idx], st);
 }
 
-int fis_advance(const fis_engine* e, int64_t steps, int32_t group, int32_t rows, int32_t* ring,
-                float* spikes_out, void* const* events, int32_t n_pairs, int32_t every,
-                void* stream) {
+int check_advance(const fis_engine* e, int64_t start, int64_t steps, int32_t group, int32_t rows,
+                  const int32_t* ring, void* const* events, int32_t n_pairs, int32_t every) {
   int rc = fis_check(e);
   if (rc) return rc;
-  if (steps < 0 || group < 1 || rows < 0 || !ring) return FIS_E_ARG;
+  if (start < 0 || steps < 0 || group < 1 || rows < 0 || !ring) return FIS_E_ARG;
   if (events && (n_pairs < 0 || every < 1)) return FIS_E_ARG;
-  const int32_t B = (rows > 0 && rows < e->batch) ? rows : e->batch;
-  const int kmax = e->p.lag < FIS_MAX_BLOCK ? e->p.lag : FIS_MAX_BLOCK;
-  cudaStream_t st = (cudaStream_t)stream;
-  int64_t left = steps;
-  int64_t launch = 0;
-  while (left > 0) {
-    const int k = (int)(left < kmax ? left : kmax);
-    float* sp = (left == k) ? spikes_out : nullptr;
-    for (int32_t g0 = 0; g0 < B; g0 += group) {
-      const int32_t nb = (B - g0) < group ? (B - g0) : group;
-      if ((rc = fis_scatter(e, g0, nb, k, ring, stream))) return rc;
-      const bool timed = events && (launch % every) == 0 && (launch / every) < n_pairs;
-      if ((rc = record_if(timed, events, 2 * (launch / every), st))) return rc;
-      if ((rc = fis_update(e, g0, nb, k, ring, sp, g0 + nb == B, stream))) return rc;
-      if ((rc = record_if(timed, events, 2 * (launch / every) + 1, st))) return rc;
-      ++launch;
-    }
-    left -= k;
-  }
   return FIS_OK;
 }
 
-}  // extern "C"
-
-namespace {
 // Per-device side stream and events of fis_advance_overlap, created on first
 // use and kept for the life of the process.
 struct OverlapRes {
   cudaStream_t side = nullptr;
-  cudaEvent_t after_sc[2] = {nullptr, nullptr};   // scatter of group gi done
-  cudaEvent_t after_upd[2] = {nullptr, nullptr};  // update of group gi done
-  cudaEvent_t block_done = nullptr;               // clock and lists of the block final
+  cudaEvent_t after_sc[2] = {nullptr, nullptr};   // scatter of launch l done (l mod 2)
+  cudaEvent_t after_upd[2] = {nullptr, nullptr};  // update of launch l done (l mod 2)
+  cudaEvent_t start = nullptr;                    // the call's starting point
 };
 constexpr int kMaxOverlapDevices = 64;
 std::mutex g_overlap_mu;  // held for a whole call: the events are shared
@@ -1107,30 +1104,83 @@ int overlap_res(OverlapRes** out) {
   if (err != cudaSuccess) return (int)err;
   if (dev < 0 || dev >= kMaxOverlapDevices) return FIS_E_ARG;
   OverlapRes& r = g_overlap[dev];
-  if (!r.block_done) {
-    if ((err = cudaStreamCreateWithFlags(&r.side, cudaStreamNonBlocking))) return (int)err;
+  if (!r.start) {
+    // The side stream gets the highest priority: the block scheduler then
+    // dispatches a scatter's CTAs as soon as update CTAs retire instead of
+    // after the whole update grid, which is what lets the two overlap.
+    int least = 0, greatest = 0;
+    if ((err = cudaDeviceGetStreamPriorityRange(&least, &greatest))) return (int)err;
+    if ((err = cudaStreamCreateWithPriority(&r.side, cudaStreamNonBlocking, greatest)))
+      return (int)err;
     for (int j = 0; j < 2; ++j) {
       if ((err = cudaEventCreateWithFlags(&r.after_sc[j], cudaEventDisableTiming)))
         return (int)err;
       if ((err = cudaEventCreateWithFlags(&r.after_upd[j], cudaEventDisableTiming)))
         return (int)err;
     }
-    if ((err = cudaEventCreateWithFlags(&r.block_done, cudaEventDisableTiming))) return (int)err;
+    if ((err = cudaEventCreateWithFlags(&r.start, cudaEventDisableTiming))) return (int)err;
   }
   *out = &r;
   return FIS_OK;
 }
+
 }  // namespace
 
 extern "C" {
 
-int fis_advance_overlap(const fis_engine* e, int64_t steps, int32_t group, int32_t rows,
-                        int32_t* ring2, float* spikes_out, void* const* events,
-                        int32_t n_pairs, int32_t every, void* stream) {
-  int rc = fis_check(e);
+int fis_scatter(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, int32_t* ring,
+                void* stream) {
+  return scatter_block(e, b0, nb, k_steps, ring, (cudaStream_t)stream, nullptr);
+}
+
+int fis_update(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, int32_t* ring,
+               float* spikes_out, int32_t last_group, void* stream) {
+  return update_block(e, b0, nb, k_steps, ring, spikes_out, last_group, (cudaStream_t)stream,
+                      nullptr);
+}
+
+int fis_block(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, int32_t* ring,
+              float* spikes_out, int32_t last_group, void* stream) {
+  const int rc = fis_scatter(e, b0, nb, k_steps, ring, stream);
   if (rc) return rc;
-  if (steps < 0 || group < 1 || rows < 0 || !ring2) return FIS_E_ARG;
-  if (events && (n_pairs < 0 || every < 1)) return FIS_E_ARG;
+  return fis_update(e, b0, nb, k_steps, ring, spikes_out, last_group, stream);
+}
+
+int fis_advance(const fis_engine* e, int64_t start, int64_t steps, int32_t group, int32_t rows,
+                int32_t* ring, float* spikes_out, void* const* events, int32_t n_pairs,
+                int32_t every, void* stream) {
+  int rc = check_advance(e, start, steps, group, rows, ring, events, n_pairs, every);
+  if (rc) return rc;
+  const int32_t B = (rows > 0 && rows < e->batch) ? rows : e->batch;
+  const int kmax = e->p.lag < FIS_MAX_BLOCK ? e->p.lag : FIS_MAX_BLOCK;
+  cudaStream_t st = (cudaStream_t)stream;
+  int64_t done = 0;
+  int64_t launch = 0;
+  while (done < steps) {
+    const int k = (int)(steps - done < kmax ? steps - done : kmax);
+    const bool final_block = done + k == steps;
+    const fis_clock clk = clock_at(e, start + done);
+    float* sp = final_block ? spikes_out : nullptr;
+    for (int32_t g0 = 0; g0 < B; g0 += group) {
+      const int32_t nb = (B - g0) < group ? (B - g0) : group;
+      const bool last = final_block && g0 + nb == B;  // advances the device clock
+      if ((rc = scatter_block(e, g0, nb, k, ring, st, &clk))) return rc;
+      const bool timed = events && (launch % every) == 0 && (launch / every) < n_pairs;
+      if ((rc = record_if(timed, events, 2 * (launch / every), st))) return rc;
+      if ((rc = update_block(e, g0, nb, k, ring, sp, last, st, &clk))) return rc;
+      if ((rc = record_if(timed, events, 2 * (launch / every) + 1, st))) return rc;
+      ++launch;
+    }
+    done += k;
+  }
+  return FIS_OK;
+}
+
+int fis_advance_overlap(const fis_engine* e, int64_t start, int64_t steps, int32_t group,
+                        int32_t rows, int32_t* ring2, float* spikes_out, void* const* events,
+                        int32_t n_pairs, int32_t every, void* stream) {
+  int rc = check_advance(e, start, steps, group, rows, ring2, events, n_pairs, every);
+  if (rc) return rc;
   const int32_t B = (rows > 0 && rows < e->batch) ? rows : e->batch;
   const int kmax = e->p.lag < FIS_MAX_BLOCK ? e->p.lag : FIS_MAX_BLOCK;
   const int32_t gmax = group < B ? group : B;
@@ -1139,36 +1189,37 @@ int fis_advance_overlap(const fis_engine* e, int64_t steps, int32_t group, int32
   OverlapRes* R = nullptr;
   if ((rc = overlap_res(&R))) return rc;
   cudaStream_t st = (cudaStream_t)stream;
-  // Scatters run on the side stream, updates on the caller's stream; group gi
-  // uses ring gi & 1, so the scatter of group gi + 1 overlaps the update of
-  // group gi.  Scatter gi waits for the update that last drained its ring
-  // (group gi - 2), or for the previous block's last update (gi < 2), which
-  // finalised the clock and the spike lists the scatter reads.
-  if ((rc = (int)cudaEventRecord(R->block_done, st))) return rc;
-  int64_t left = steps;
+  // Scatters run on the side stream, updates on the caller's stream, launch
+  // l (over all blocks and groups, in order) using ring l mod 2.  Scatter l
+  // waits only for update l - 2, which drained its ring and -- updates
+  // running in order -- also wrote every spike list the scatter reads (those
+  // of the same trial group one block earlier); so each update overlaps the
+  // scatter of the next launch, across block boundaries too.
+  if ((rc = (int)cudaEventRecord(R->start, st))) return rc;
+  int64_t done = 0;
   int64_t launch = 0;
-  while (left > 0) {
-    const int k = (int)(left < kmax ? left : kmax);
-    float* sp = (left == k) ? spikes_out : nullptr;
-    int gi = 0;
-    for (int32_t g0 = 0; g0 < B; g0 += group, ++gi) {
+  while (done < steps) {
+    const int k = (int)(steps - done < kmax ? steps - done : kmax);
+    const bool final_block = done + k == steps;
+    const fis_clock clk = clock_at(e, start + done);
+    float* sp = final_block ? spikes_out : nullptr;
+    for (int32_t g0 = 0; g0 < B; g0 += group) {
       const int32_t nb = (B - g0) < group ? (B - g0) : group;
-      const bool last = g0 + nb == B;
-      int32_t* ring = rings[gi & 1];
-      cudaEvent_t dep = gi >= 2 ? R->after_upd[gi & 1] : R->block_done;
+      const bool last = final_block && g0 + nb == B;  // advances the device clock
+      const int r = (int)(launch & 1);
+      cudaEvent_t dep = launch >= 2 ? R->after_upd[r] : R->start;
       if ((rc = (int)cudaStreamWaitEvent(R->side, dep, 0))) return rc;
-      if ((rc = fis_scatter(e, g0, nb, k, ring, R->side))) return rc;
-      if ((rc = (int)cudaEventRecord(R->after_sc[gi & 1], R->side))) return rc;
-      if ((rc = (int)cudaStreamWaitEvent(st, R->after_sc[gi & 1], 0))) return rc;
+      if ((rc = scatter_block(e, g0, nb, k, rings[r], R->side, &clk))) return rc;
+      if ((rc = (int)cudaEventRecord(R->after_sc[r], R->side))) return rc;
+      if ((rc = (int)cudaStreamWaitEvent(st, R->after_sc[r], 0))) return rc;
       const bool timed = events && (launch % every) == 0 && (launch / every) < n_pairs;
       if ((rc = record_if(timed, events, 2 * (launch / every), st))) return rc;
-      if ((rc = fis_update(e, g0, nb, k, ring, sp, last, stream))) return rc;
+      if ((rc = update_block(e, g0, nb, k, rings[r], sp, last, st, &clk))) return rc;
       if ((rc = record_if(timed, events, 2 * (launch / every) + 1, st))) return rc;
-      if ((rc = (int)cudaEventRecord(last ? R->block_done : R->after_upd[gi & 1], st)))
-        return rc;
+      if ((rc = (int)cudaEventRecord(R->after_upd[r], st))) return rc;
       ++launch;
     }
-    left -= k;
+    done += k;
   }
   return FIS_OK;
 }

@@ -17,7 +17,7 @@ PKG = Path(__file__).resolve().parent
 LIB_NAME = "libfis_b200.so"
 LIB_PATH = PKG / LIB_NAME
 
-FIS_ABI_VERSION = 3
+FIS_ABI_VERSION = 4
 FIS_MAX_BLOCK = 20
 FIS_NOALLOC_RING_INTS = 3 << 20
 REF_EV_ABI = 3
@@ -106,8 +106,8 @@ def load(path=None):
     L.fis_check.argtypes = [P]
     L.fis_block.argtypes = [P, I32, I32, I32, P, P, I32, P]
     L.fis_scatter.argtypes = [P, I32, I32, I32, P, P]
-    L.fis_advance.argtypes = [P, I64, I32, I32, P, P, P, I32, I32, P]
-    L.fis_advance_overlap.argtypes = [P, I64, I32, I32, P, P, P, I32, I32, P]
+    L.fis_advance.argtypes = [P, I64, I64, I32, I32, P, P, P, I32, I32, P]
+    L.fis_advance_overlap.argtypes = [P, I64, I64, I32, I32, P, P, P, I32, I32, P]
     L.fis_update.argtypes = [P, I32, I32, I32, P, P, I32, P]
     L.fis_delay_buffer.argtypes = [P, I32, I32, P, P, P]
     L.fis_spikes_f32.argtypes = [P, I32, I32, I64, P, P]

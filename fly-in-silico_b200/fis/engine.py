@@ -362,7 +362,7 @@ class Core:
         fn, name = self.lib.fis_advance, "fis_advance"
         if self.overlap and nrows > self.group:
             fn, name = self.lib.fis_advance_overlap, "fis_advance_overlap"
-        rc = fn(ctypes.byref(self.desc), steps, self.group, nrows,
+        rc = fn(ctypes.byref(self.desc), self.step, steps, self.group, nrows,
                 ctypes.c_void_p(self.ring2.data_ptr()),
                 ctypes.c_void_p(spikes_out.data_ptr()) if spikes_out is not None else None,
                 ev_arr, n_pairs, max(1, int(every)), ctypes.c_void_p(st.cuda_stream))

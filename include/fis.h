@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define FIS_ABI_VERSION 3
+#define FIS_ABI_VERSION 4
 
 /* Largest number of steps one block may advance (registers per thread). */
 #define FIS_MAX_BLOCK 20
@@ -229,7 +229,10 @@ int fis_update(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps,
  * min(FIS_MAX_BLOCK, lag) steps (the last one shorter), each block running
  * fis_scatter + fis_update for the trial groups [g0, g0+group) in turn.  The
  * native form of a host loop over fis_block.  Slots at or above `rows` must
- * not be running (their trials ended); they stay frozen.
+ * not be running (their trials ended); they stay frozen.  `start` is the
+ * device clock's step on entry: every launch is given its block's step, so
+ * no launch waits for the clock, which the call's last launch advances to
+ * start + steps.
  *   ring        scratch ring of fis_block's layout for min(FIS_MAX_BLOCK,
  *               lag) slots and `group` trials, empty on entry and on return
  *   spikes_out  float [B][N] or NULL, written by the last block
@@ -237,24 +240,24 @@ int fis_update(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps,
  *               around the update launch number j*every (0-based over the
  *               whole call), for timing the dominant kernel
  */
-int fis_advance(const fis_engine* e, int64_t steps, int32_t group, int32_t rows,
-                int32_t* ring, float* spikes_out, void* const* events,
+int fis_advance(const fis_engine* e, int64_t start, int64_t steps, int32_t group,
+                int32_t rows, int32_t* ring, float* spikes_out, void* const* events,
                 int32_t n_pairs, int32_t every, void* stream);
 
 /*
- * fis_advance with two scratch rings, so that the scatter of trial group
- * gi + 1 (on a library-owned side stream, one per device) runs while the
- * update of group gi runs on `stream`; group gi uses ring gi mod 2.  Ordered
- * by events: every scatter waits for the update that last drained its ring,
- * and the first two of a block for the previous block's last update.  On
- * return all work is ordered before later work on `stream`.
+ * fis_advance with two scratch rings, so that each scatter (on a
+ * library-owned side stream, one per device) runs while the previous update
+ * runs on `stream`, across block boundaries too: launch l (over all blocks
+ * and groups, in order) uses ring l mod 2 and its scatter waits only for
+ * update l - 2.  On return all work is ordered before later work on
+ * `stream`.
  *   ring2  two consecutive rings of fis_block's layout, each for
  *          min(FIS_MAX_BLOCK, lag) slots and min(group, rows or batch)
  *          trials, empty on entry and on return
  * Other arguments as fis_advance.  Calls are serialised inside the library.
  */
-int fis_advance_overlap(const fis_engine* e, int64_t steps, int32_t group, int32_t rows,
-                        int32_t* ring2, float* spikes_out, void* const* events,
+int fis_advance_overlap(const fis_engine* e, int64_t start, int64_t steps, int32_t group,
+                        int32_t rows, int32_t* ring2, float* spikes_out, void* const* events,
                         int32_t n_pairs, int32_t every, void* stream);
 
 /*
