@@ -432,7 +432,7 @@ __device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
 struct Pair {
   f2 v, g, r;        // membrane, conductance, refractory counter
   f2 keep;           // 1 - spike of the previous step
-  f2 m_in, m_hold, v_hold;
+  f2 m_hold, v_hold;
   float rs0, rs1;    // refractory steps (0 for driven neurons)
   float vth0, vth1;  // threshold; +inf under the fire mask (see lif_step2)
 };
@@ -450,19 +450,27 @@ __device__ __forceinline__ f2 subp(const Consts& C, f2 c, f2 p) { return fma2(p,
 // One step of sim.py:921-952 for the neuron in both trials, the reference's
 // operation order one rounding at a time.  f0/f1: the spikes; sp: them as
 // floats.
-__device__ __forceinline__ void lif_step2(Pair& s, const Consts& C, float c0, float c1, f2 vstim,
-                                          bool& f0, bool& f1, f2& sp) {
+//
+// c0/c1 are the step's delayed input counts, already zero where the input
+// mask m_in is 0 (and for a silenced neuron, which has no incoming synapses,
+// sim.py:324-336).  The reference forms (w * count) * m_in * gate and adds it
+// to g * a_syn; here the refractory gate and m_in select the count itself
+// and w * count is added.  Where both factors are 1 the products are the
+// same bits; where one is 0 the reference adds a signed zero and this adds
+// +0, which can change only the sign of a zero sum -- and the conductance
+// reset below, gn - gn * spike, turns either zero into +0.  So the stored
+// state is the same bits, for two multiplies fewer per step.
+__device__ __forceinline__ void lif_step2(Pair& s, const Consts& C, int32_t c0, int32_t c1,
+                                          f2 vstim, bool& f0, bool& f1, f2& sp) {
   // refractory counter and gate (sim.py:921-923); r is the previous step's
   // product, so its increment is an addp
   s.r = mul2(addp(C, s.r, C.one), s.keep);
   float r0, r1;
   up2(s.r, r0, r1);
-  const f2 gate = pk2(r0 >= s.rs0 ? 1.f : 0.f, r1 >= s.rs1 ? 1.f : 0.f);
-  // delayed input and the new conductance (sim.py:928-929); the counts
-  // arrive already zero for a silenced neuron (no incoming synapses,
-  // sim.py:324-336)
-  const f2 delayed = mul2(mul2(C.w, pk2(c0, c1)), s.m_in);
-  const f2 gn = addp(C, mul2(s.g, C.a_syn), mul2(delayed, gate));
+  const int32_t g0 = r0 >= s.rs0 ? c0 : 0, g1 = r1 >= s.rs1 ? c1 : 0;
+  // delayed input and the new conductance (sim.py:928-929)
+  const f2 delayed = mul2(C.w, pk2(__int2float_rn(g0), __int2float_rn(g1)));
+  const f2 gn = addp(C, mul2(s.g, C.a_syn), delayed);
   // membrane with the previous conductance (sim.py:936-938)
   f2 v = add2(s.v, vstim);
   v = addp(C, mul2(C.a_mem, sub2(s.g, sub2(v, C.v_rest))), v);
@@ -484,7 +492,7 @@ __device__ __forceinline__ void lif_step2(Pair& s, const Consts& C, float c0, fl
 // ring, trial A's biased count in the low half and trial B's in the high
 // half; flipping each half's top bit turns 0x8000 + c into c as an int16.
 // Otherwise two int32 columns, one per trial.  `mask` zeroes the counts of a
-// silenced neuron, per trial.
+// silenced neuron and of one whose input mask is off, per trial.
 struct Staged2 {
   const int32_t* col;  // this thread's word of slot 0 (kHalf) or of trial A's row
   uint32_t mask0, mask1;
@@ -497,14 +505,14 @@ struct StagedRow {
 };
 
 template <bool kHalf>
-__device__ __forceinline__ void staged2(const Staged2& s, int k, float& c0, float& c1) {
+__device__ __forceinline__ void staged2(const Staged2& s, int k, int32_t& c0, int32_t& c1) {
   if (kHalf) {
     const uint32_t w = ((uint32_t)s.col[k * kTile] ^ kEmptyPair) & (s.mask0 | s.mask1);
-    c0 = __int2float_rn((int32_t)(int16_t)(w & 0xFFFFu));
-    c1 = __int2float_rn((int32_t)(int16_t)(w >> 16));
+    c0 = (int32_t)(int16_t)(w & 0xFFFFu);
+    c1 = (int32_t)w >> 16;
   } else {
-    c0 = __int2float_rn((int32_t)((uint32_t)s.col[k * 2 * kTile] & s.mask0));
-    c1 = __int2float_rn((int32_t)((uint32_t)s.col[k * 2 * kTile + kTile] & s.mask1));
+    c0 = (int32_t)((uint32_t)s.col[k * 2 * kTile] & s.mask0);
+    c1 = (int32_t)((uint32_t)s.col[k * 2 * kTile + kTile] & s.mask1);
   }
 }
 
@@ -512,9 +520,10 @@ __device__ __forceinline__ void staged2(const Staged2& s, int k, float& c0, floa
 // is driven in either trial, so warps without drive carry no drive logic.
 // `kPartial`: a trial starts or ends inside this block (or only one of the
 // two runs), so each step commits only the lanes whose trial runs at that
-// step.  Returns the fired steps of each trial as bits, the last step in bit
-// 0 (exact in float).
-template <bool kTape, bool kDrive, bool kHalf, bool kPartial>
+// step.  `kRaster`: store every step's raster words (else the caller keeps
+// only the last step's).  Returns the fired steps of each trial as bits, the
+// last step in bit 0 (exact in float).
+template <bool kTape, bool kDrive, bool kHalf, bool kPartial, bool kRaster = true>
 __device__ __forceinline__ f2 step_loop2(Pair& st, const Consts& C, const fis_engine& E, int K,
                                          int ka0, int kb0, int ka1, int kb1, uint32_t dm0,
                                          uint32_t dm1, const Staged2& in, uint32_t* sbal0,
@@ -531,7 +540,7 @@ __device__ __forceinline__ f2 step_loop2(Pair& st, const Consts& C, const fis_en
   // needs no lane predicate.
 #pragma unroll(kPartial ? 1 : 2)
   for (int k = 0; k < K; ++k) {
-    float c0, c1;
+    int32_t c0, c1;
     staged2<kHalf>(in, k, c0, c1);
     f2 vstim = pk2(0.f, 0.f);
     if (kTape) {
@@ -561,8 +570,10 @@ __device__ __forceinline__ f2 step_loop2(Pair& st, const Consts& C, const fis_en
     } else {
       lif_step2(st, C, c0, c1, vstim, f0, f1, sp);
     }
-    sbal0[k] = __ballot_sync(0xFFFFFFFFu, f0);
-    sbal1[k] = __ballot_sync(0xFFFFFFFFu, f1);
+    if (kRaster) {
+      sbal0[k] = __ballot_sync(0xFFFFFFFFu, f0);
+      sbal1[k] = __ballot_sync(0xFFFFFFFFu, f1);
+    }
     nspk = fma2(nspk, two, sp);
   }
   return nspk;
@@ -714,13 +725,12 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
 
   if (runs[0] || runs[1]) {
   Pair st;
-  float vth[2], rs[2], min_[2], mhold[2], vhold[2];
+  float vth[2], rs[2], mhold[2], vhold[2];
 #pragma unroll
   for (int t = 0; t < 2; ++t) {
     const bool on = runs[t] && valid && !(fl[t] & FIS_FL_FIRE_OFF);
     vth[t] = on ? E.p.v_th : __int_as_float(0x7f800000);
     rs[t] = (fl[t] & FIS_FL_NOREFRAC) ? 0.f : E.p.refrac_steps;
-    min_[t] = (fl[t] & FIS_FL_IN_OFF) ? 0.f : 1.f;
     const bool hold = fl[t] & FIS_FL_HOLD;
     mhold[t] = hold ? 0.f : 1.f;
     vhold[t] = hold ? tr[t].v_clamp : 0.f;
@@ -729,7 +739,6 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
   st.g = pk2(gg[0], gg[1]);
   st.r = pk2(rr[0], rr[1]);
   st.keep = pk2(s_prev[0] ? 0.f : 1.f, s_prev[1] ? 0.f : 1.f);
-  st.m_in = pk2(min_[0], min_[1]);
   st.m_hold = pk2(mhold[0], mhold[1]);
   st.v_hold = pk2(vhold[0], vhold[1]);
   st.rs0 = rs[0];
@@ -749,8 +758,8 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
   // trials and on the warp's vote only), so every lane reaches each ballot.
   Staged2 in;
   in.col = &sring[0][threadIdx.x];
-  in.mask0 = (fl[0] & FIS_FL_SILENCED) ? 0u : (kHalf ? 0x0000FFFFu : 0xFFFFFFFFu);
-  in.mask1 = (fl[1] & FIS_FL_SILENCED) ? 0u : (kHalf ? 0xFFFF0000u : 0xFFFFFFFFu);
+  in.mask0 = (fl[0] & (FIS_FL_SILENCED | FIS_FL_IN_OFF)) ? 0u : (kHalf ? 0x0000FFFFu : 0xFFFFFFFFu);
+  in.mask1 = (fl[1] & (FIS_FL_SILENCED | FIS_FL_IN_OFF)) ? 0u : (kHalf ? 0xFFFF0000u : 0xFFFFFFFFu);
   // A trial slot that does not run is inert in the lanes it shares (never
   // fires, never stored), so only a trial that starts or ends inside the
   // block needs the per-step commit of the partial loop.
@@ -768,12 +777,32 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
                                                runs[0] ? kb[0] : 0, runs[1] ? ka[1] : 0,
                                                runs[1] ? kb[1] : 0, dm[0], dm[1], in, sb0, sb1,
                                                sidx[0], sidx[1], valid);
-  else if (warp_driven)
+  else if (E.raster && warp_driven)
     nspk = step_loop2<false, true, kHalf, false>(st, C, E, K, 0, K, 0, K, dm[0], dm[1], in, sb0,
                                                 sb1, sidx[0], sidx[1], valid);
-  else
+  else if (E.raster)
     nspk = step_loop2<false, false, kHalf, false>(st, C, E, K, 0, K, 0, K, 0u, 0u, in, sb0, sb1,
                                                  sidx[0], sidx[1], valid);
+  else if (warp_driven)
+    nspk = step_loop2<false, true, kHalf, false, false>(st, C, E, K, 0, K, 0, K, dm[0], dm[1], in,
+                                                       sb0, sb1, sidx[0], sidx[1], valid);
+  else
+    nspk = step_loop2<false, false, kHalf, false, false>(st, C, E, K, 0, K, 0, K, 0u, 0u, in,
+                                                        sb0, sb1, sidx[0], sidx[1], valid);
+  // Without the full raster only the last step's words are kept (the next
+  // block reads them for the refractory reset); the partial and tape loops
+  // always store every step.
+  const bool only_last = !E.raster && full && !kTape;
+  if (only_last) {
+    float k0, k1;
+    up2(st.keep, k0, k1);
+    const uint32_t w0 = __ballot_sync(0xFFFFFFFFu, k0 == 0.f);
+    const uint32_t w1 = __ballot_sync(0xFFFFFFFFu, k1 == 0.f);
+    if (lane == 0) {
+      sb0[K - 1] = w0;
+      sb1[K - 1] = w1;
+    }
+  }
   __syncwarp();
 
   float ov[2], og[2], orr[2], okeep[2], ospk[2];
@@ -787,7 +816,7 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
     if (!runs[t]) continue;
     const int b = b0 + 2 * pp + t;
     // the raster words of the K steps into the ring of the last L steps
-    if (lane < K && warp_valid) {
+    if ((only_last ? lane == K - 1 : lane < K) && warp_valid) {
       const int sl = slot0 + lane < L ? slot0 + lane : slot0 + lane - L;
       bitrow[t][sl] = sbal[t][wib][lane];
     }

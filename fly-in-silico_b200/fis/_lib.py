@@ -17,7 +17,7 @@ PKG = Path(__file__).resolve().parent
 LIB_NAME = "libfis_b200.so"
 LIB_PATH = PKG / LIB_NAME
 
-FIS_ABI_VERSION = 4
+FIS_ABI_VERSION = 5
 FIS_MAX_BLOCK = 20
 FIS_NOALLOC_RING_INTS = 3 << 20
 REF_EV_ABI = 3
@@ -76,7 +76,7 @@ class EngineDesc(ctypes.Structure):
                 ("batch", ctypes.c_int32), ("chunk", ctypes.c_int32),
                 ("n_recs", ctypes.c_int32), ("ring16", ctypes.c_int32),
                 ("wait_polls", ctypes.c_uint32), ("inject_stall", ctypes.c_uint32),
-                ("pad_", ctypes.c_int32), ("p", LifParams)]
+                ("raster", ctypes.c_int32), ("p", LifParams)]
 
 
 _lib = None

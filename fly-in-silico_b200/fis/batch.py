@@ -79,8 +79,9 @@ class Batch:
 
     def __init__(self, conn: Connectome, capacity: int, params=None, device="cuda",
                  group=None, chunk=None, core: Core | None = None):
+        # results come from recordings: no per-step raster needed
         self.core = core or Core(conn, capacity, params=params, device=device, group=group,
-                                 chunk=chunk)
+                                 chunk=chunk, raster=False)
         self.n = self.core.n
         self.capacity = self.core.batch
         self._recs = {}                          # index -> int32 [n_bins][N]

@@ -83,7 +83,7 @@ class Core:
 
     def __init__(self, conn: Connectome, batch: int, params=None, device="cuda",
                  group=None, chunk=None, max_block=_lib.FIS_MAX_BLOCK, ring=None,
-                 overlap=True):
+                 overlap=True, raster=True):
         self.device = require_cuda(device)
         self.lib = _lib.load()
         conn.check_bounds()
@@ -94,6 +94,9 @@ class Core:
                 "exact for this matrix" % ex["max_abs_row_sum"])
         self.conn = conn
         self.overlap = bool(overlap)
+        # raster=False keeps only each block's last step in `bits` (enough for
+        # the next block); spikes of other steps are then not available
+        self.raster = bool(raster)
         # Scratch-ring element: biased int16 when no neuron's incoming
         # |count| sum reaches 2**15 (exact, half the ring traffic), else int32.
         ring = ring or os.environ.get("FIS_RING", "auto")
@@ -189,6 +192,7 @@ class Core:
         d.list_cap = self.list_cap
         d.n, d.batch, d.chunk, d.n_recs = n, B, self.chunk, 0
         d.ring16 = 1 if self.ring16 else 0
+        d.raster = 1 if self.raster else 0
         d.p = self.P
         _lib.check(self.lib.fis_check(ctypes.byref(d)), "fis_check")
 
@@ -380,6 +384,8 @@ class Core:
         step = self.step - 1 if step is None else int(step)
         if not (self.step - self.lag <= step < self.step) or step < 0:
             raise ValueError("step %d is not among the last %d" % (step, self.lag))
+        if not self.raster and step != self.step - 1:
+            raise ValueError("this core keeps the raster of its last step only (raster=False)")
         if out is None:
             out = torch.empty((self.batch, self.n), dtype=torch.float32, device=self.device)
         rc = self.lib.fis_spikes_f32(ctypes.byref(self.desc), 0, self.batch, step,

@@ -94,7 +94,7 @@ def tune(conn: Connectome, batch: int, params=None, groups=None, chunks=None, st
                               | {batch})
     results = []
     for chunk in chunks:
-        core = Core(conn, batch, params=params, chunk=chunk, group=groups[0])
+        core = Core(conn, batch, params=params, chunk=chunk, group=groups[0], raster=False)
         _mix(core)
         for g in groups:
             core.set_group(g)

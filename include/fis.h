@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define FIS_ABI_VERSION 4
+#define FIS_ABI_VERSION 5
 
 /* Largest number of steps one block may advance (registers per thread). */
 #define FIS_MAX_BLOCK 20
@@ -150,7 +150,10 @@ typedef struct fis_engine {
                             polls; 0 = the default (~4M, far above any copy) */
   uint32_t inject_stall; /* test hook: nonzero = issue no staging copy, so
                             every wait runs out and sets FIS_ERR_STAGE       */
-  int32_t pad_;
+  int32_t raster;     /* nonzero: keep the raster of every step in `bits`;
+                         0: only of each block's last step (all the next
+                         block needs), for runs that read spikes through
+                         recordings and spike lists alone                  */
   fis_lif_params p;
 } fis_engine;
 

@@ -144,3 +144,24 @@ def test_bounded_wait_reports_error_and_context_survives():
     fresh = Batch(c, 2, group=2).run(sp)
     for j, s in enumerate(sp):
         assert np.array_equal(fresh[j], oracle_trial(c, s)[1]), j
+
+
+def test_last_step_raster_mode_keeps_state_and_last_spikes():
+    """raster=False (only each block's last step kept) changes nothing else."""
+    from fis.batch import Batch
+    from fis.engine import Core
+
+    c = conn()
+    sp = specs(81, 4, (90, 140))
+    got = []
+    for raster in (True, False):
+        core = Core(c, 4, group=2, raster=raster)
+        counts = Batch(c, 4, core=core).run(sp)
+        last = core.spikes_at().cpu().numpy()
+        got.append((counts, core.v.cpu().numpy(), core.g.cpu().numpy(),
+                    core.refrac.cpu().numpy(), last))
+        if not raster:
+            with pytest.raises(ValueError):
+                core.spikes_at(core.step - 2)
+    for a, b in zip(got[0], got[1]):
+        assert np.array_equal(a, b)
