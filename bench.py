@@ -340,8 +340,6 @@ def main():
     value = world * units_rank * args.steps / (ms / 1000.0)
 
     # end to end through the public API: host specs in, host counts out
-    h2d = args.trials * conn.n * (1 + 4) + args.trials * 48 + args.trials * 8
-    d2h = args.trials * conn.n * 4
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
@@ -349,6 +347,10 @@ def main():
     barrier()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e = world * units_rank * args.steps / e2e_s
+    # bytes copied per run: the sparse trial rows, the trial table and the
+    # recording pointer table in; the per-trial counts out
+    h2d = batch.last_h2d_bytes + args.trials * 48 + 8 * len(batch.recordings())
+    d2h = batch.last_d2h_bytes
 
     # the plain single-trial step through the reference-compatible API
     plain = None

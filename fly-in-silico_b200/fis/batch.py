@@ -68,6 +68,48 @@ def host_rows(specs, n):
     return flags, rates
 
 
+def sparse_rows(specs, n, slots):
+    """The non-zero flags and rates of ``specs`` placed in ``slots``, sparse.
+
+    Returns (flag_at, flag_bits, rate_at, rate_val): flat positions
+    slot * n + neuron (int64, unique, ascending) with the OR of their flag bits
+    (uint8), and the positions with a rate (int64, unique) with the rate as
+    float32 (a repeated stimulated neuron keeps its last rate, as an indexed
+    assignment does).  Together they equal ``host_rows`` laid into the slots.
+    """
+    f_at, f_bits, r_at, r_val = [], [], [], []
+    for j, (b, s) in enumerate(zip(slots, specs)):
+        base = int(b) * n
+        stim = np.asarray(s.stim, dtype=np.int64)
+        r = np.asarray(s.rate_hz, dtype=np.float64)
+        check_rates_hz(r, "trial %d rate" % j)
+        r_at.append(base + stim)
+        r_val.append(np.broadcast_to(r.astype(np.float32), stim.shape))
+        nore = stim if s.no_refractory is None else np.asarray(s.no_refractory, np.int64)
+        for idx, bit in ((nore, _lib.FIS_FL_NOREFRAC), (s.silenced, _lib.FIS_FL_SILENCED),
+                         (s.fire_off, _lib.FIS_FL_FIRE_OFF), (s.out_off, _lib.FIS_FL_OUT_OFF),
+                         (s.in_off, _lib.FIS_FL_IN_OFF), (s.hold, _lib.FIS_FL_HOLD)):
+            if idx is not None and len(idx):
+                idx = np.asarray(idx, np.int64)
+                f_at.append(base + idx)
+                f_bits.append(np.full(idx.shape, bit, dtype=np.uint8))
+    i64, u8, f32 = np.zeros(0, np.int64), np.zeros(0, np.uint8), np.zeros(0, np.float32)
+    fa = np.concatenate(f_at) if f_at else i64
+    fb = np.concatenate(f_bits) if f_bits else u8
+    ra = np.concatenate(r_at) if r_at else i64
+    rv = np.concatenate(r_val) if r_val else f32
+    if fa.size:
+        order = np.argsort(fa, kind="stable")
+        fa, fb = fa[order], fb[order]
+        fa, first = np.unique(fa, return_index=True)
+        fb = np.bitwise_or.reduceat(fb, first)
+    if ra.size:  # keep the last of repeated positions
+        rev_at, rev_first = np.unique(ra[::-1], return_index=True)
+        rv = rv[::-1][rev_first]
+        ra = rev_at
+    return fa, fb, ra, rv
+
+
 class Batch:
     """Trial slots on one GPU; load specs, advance, read per-trial results.
 
@@ -136,48 +178,63 @@ class Batch:
     def load(self, slots, specs, start=None, rec=None):
         """Place ``specs`` into ``slots`` starting at global step ``start``.
 
-        Rows are built on the host and copied once (pinned, asynchronous);
-        state is reset to the reference's initial values.  ``rec``: a shared
-        recording buffer for all these trials; by default each trial gets one
-        of its own.
+        The trials' non-zero flags and rates travel sparse (positions and
+        values, one pinned copy) and are laid into the zeroed rows on the
+        device; state is reset to the reference's initial values.  ``rec``: a
+        shared recording buffer for all these trials; by default each trial
+        gets one of its own (views of one buffer when their bin counts agree).
         """
         c = self.core
         slots = list(slots)
+        k = len(slots)
         start = c.step if start is None else int(start)
-        flags, rates = host_rows(specs, self.n)
-        fpin = self._staging("flags", flags.shape, torch.uint8)
-        rpin = self._staging("rates", rates.shape, torch.float32)
-        fpin.numpy()[:] = flags
-        rpin.numpy()[:] = rates
+        fa, fb, ra, rv = sparse_rows(specs, self.n, slots)
+        # one pinned staging buffer: int64 positions first (8-byte aligned), then
+        # float32 rates, then uint8 flag bits
+        nbytes = 8 * (fa.size + ra.size) + 4 * rv.size + fb.size
+        pin = self._staging("rows", (max(8, -(-nbytes // 8) * 8),), torch.uint8)
+        host = pin.numpy()
+        o1, o2 = 8 * fa.size, 8 * (fa.size + ra.size)
+        o3 = o2 + 4 * rv.size
+        host[:o1].view(np.int64)[:] = fa
+        host[o1:o2].view(np.int64)[:] = ra
+        host[o2:o3].view(np.float32)[:] = rv
+        host[o3:o3 + fb.size] = fb
+        dev = pin[:nbytes].to(c.device, non_blocking=True)
+        self.last_h2d_bytes = nbytes
         idx = torch.as_tensor(slots, dtype=torch.long, device=c.device)
-        contiguous = slots == list(range(slots[0], slots[0] + len(slots)))
-        rows = slice(slots[0], slots[0] + len(slots)) if contiguous else idx
-        if contiguous:
-            c.flags[rows].copy_(fpin, non_blocking=True)
-            c.rates[rows].copy_(rpin, non_blocking=True)
-        else:
-            c.flags[idx] = fpin.to(c.device, non_blocking=True)
-            c.rates[idx] = rpin.to(c.device, non_blocking=True)
+        contiguous = slots == list(range(slots[0], slots[0] + k))
+        rows = slice(slots[0], slots[0] + k) if contiguous else idx
+        c.flags[rows] = 0
+        c.rates[rows] = 0.0
+        if fa.size:
+            c.flags.view(-1)[dev[:o1].view(torch.int64)] = dev[o3:o3 + fb.size]
+        if ra.size:
+            c.rates.view(-1)[dev[o1:o2].view(torch.int64)] = dev[o2:o3].view(torch.float32)
         for b in slots:
             if self._slot_rec[b] is not None:
                 self.release(b)
         shared = None
         if rec is not None:
-            shared = self._rec_add(rec, len(slots))
-        for b, s in zip(slots, specs):
+            shared = self._rec_add(rec, k)
+        bins = [s.n_bins() for s in specs]
+        own = None
+        if shared is None and len(set(bins)) == 1:
+            own = torch.zeros((k, bins[0], self.n), dtype=torch.int32, device=c.device)
+        self.last_recording = own  # [k][n_bins][N] in the order of `specs`, or None
+        for j, (b, s) in enumerate(zip(slots, specs)):
             t = c.trials[b]
             t.seed = int(s.seed) & (2 ** 64 - 1)
             t.stream = 0
             t.start = start
             t.end = start + int(s.steps)
             t.v_clamp = float(np.float32(c.pdict["vReset"] if s.v_clamp is None else s.v_clamp))
-            if shared is None:
-                r = torch.zeros((s.n_bins(), self.n), dtype=torch.int32, device=c.device)
-                ri = self._rec_add(r, 1)
-                nb = s.n_bins()
+            if shared is not None:
+                ri, nb = shared, int(rec.shape[0])
             else:
-                ri = shared
-                nb = int(rec.shape[0])
+                r = own[j] if own is not None else torch.zeros(
+                    (bins[j], self.n), dtype=torch.int32, device=c.device)
+                ri, nb = self._rec_add(r, 1), bins[j]
             self._slot_rec[b] = ri
             t.rec = ri
             t.bin_steps = int(s.bin_steps or max(1, s.steps))
@@ -217,9 +274,15 @@ class Batch:
             c.advance(nxt - t, timer=timer, rows=rows)
             t = nxt
         out = self._staging("counts", (k, self.n), torch.int32)
-        dev = torch.stack([self.recording(self.slots_of_run[j]).sum(0, dtype=torch.int32)
-                           for j in range(k)])
+        if self.last_recording is not None:  # [k][n_bins][N], trials in slot order
+            sums = self.last_recording.sum(1, dtype=torch.int32)
+            pos = torch.as_tensor(self.slots_of_run, dtype=torch.long, device=c.device)
+            dev = sums.index_select(0, pos)
+        else:
+            dev = torch.stack([self.recording(self.slots_of_run[j]).sum(0, dtype=torch.int32)
+                               for j in range(k)])
         out.copy_(dev, non_blocking=True)
+        self.last_d2h_bytes = out.numel() * out.element_size()
         torch.cuda.current_stream(c.device).synchronize()
         c.check_errors()
         return out.numpy().copy()

@@ -137,3 +137,26 @@ def test_engine_refuses_cpu_loudly():
     c = C.synthetic(n=500, e=20000, seed=1, cache=False)
     with pytest.raises(evspmv.EventKernelUnavailable):
         sim.Engine(c, c.n, device="cpu")
+
+
+def test_sparse_rows_equal_dense_rows():
+    """The sparse upload of Batch.load lays out exactly host_rows' rows."""
+    from fis.batch import host_rows, random_specs, sparse_rows
+
+    n = 5000
+    specs = random_specs(n, 6, 3, 100, stim_range=(50, 300), silenced_range=(1, 40))
+    specs[2].fire_off = specs[2].stim[:10]
+    specs[3].hold, specs[3].in_off = np.arange(10, 60), np.arange(30, 90)
+    specs[4].stim = np.concatenate([specs[4].stim, specs[4].stim[:5]])   # repeats
+    specs[4].rate_hz = np.arange(len(specs[4].stim), dtype=np.float64) + 1.0
+    specs[5].out_off = specs[5].stim[:7]
+    slots = [3, 0, 5, 1, 4, 2]
+    flags, rates = host_rows(specs, n)
+    fa, fb, ra, rv = sparse_rows(specs, n, slots)
+    assert np.all(np.diff(fa) > 0) and np.all(np.diff(ra) > 0)
+    F = np.zeros((6, n), np.uint8)
+    R = np.zeros((6, n), np.float32)
+    F.reshape(-1)[fa] = fb
+    R.reshape(-1)[ra] = rv
+    for j, b in enumerate(slots):
+        assert np.array_equal(F[b], flags[j]) and np.array_equal(R[b], rates[j]), j
