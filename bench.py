@@ -41,11 +41,16 @@ SPEC_SEED = 2024
 CONN_SEED = 0
 # Update-kernel DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum)
 # per trial-neuron and block, from the ncu capture summarised in
-# profiles/k_update_batched64.md (74.7 MB for one launch of 8 trials x 138,639
-# neurons x 20 steps; ncu flushes caches between replay passes, so this counts
-# the scratch ring as cold reads and is an upper bound).  Scaled to the
-# bench's launch size by the neurons it processes.
-NCU_TRAFFIC_PER_NEURON_BLOCK = 74.75e6 / (8 * 138_639)
+# profiles/k_update_batched64.md (206.5 MB for one launch of 16 trials x
+# 138,639 neurons x 20 steps at steady activity; ncu flushes caches between
+# replay passes, so this counts the L2-resident scratch ring as cold reads and
+# its clearing as DRAM writes, an upper bound).  Scaled to the bench's launch
+# size by the neurons it processes.
+NCU_TRAFFIC_PER_NEURON_BLOCK = 206.47e6 / (16 * 138_639)
+# Algorithmic HBM bytes of the update per trial-neuron and block: state
+# v, g, refrac read and written (24), flags (1), rates (4), kick steps (4),
+# and the previous and last step's raster bits (2/8).
+UPDATE_BYTES_PER_NEURON_BLOCK = 24 + 1 + 4 + 4 + 2 / 8
 
 
 def parse():
@@ -384,7 +389,7 @@ def main():
     roof = None
     if upd_ms:
         G = core.group
-        bytes_launch = G * conn.n * (4 * 3 * 2 + 1 + 4) + G * conn.n * (core.max_block + 1) / 8
+        bytes_launch = G * conn.n * UPDATE_BYTES_PER_NEURON_BLOCK
         alg = bytes_launch
         achieved = bytes_launch / (upd_ms / 1000.0) / 1e9
         roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",

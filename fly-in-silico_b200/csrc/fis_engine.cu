@@ -1063,7 +1063,10 @@ int scatter_block(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, 
   A.clk_given = clk ? 1 : 0;
   if (clk) A.clk = *clk;
   const size_t smem = sizeof(int32_t) * (size_t)((k_steps + 1) * nb + 1);
-  k_scatter<<<sm_count() * 8, kScatThreads, smem, st>>>(*e, A);
+  // up to 8 CTAs per SM; fewer for small blocks (one trial, one step), where
+  // the spikes of a step fill one pass of a CTA per SM
+  const int per_sm = std::min(8, std::max(1, nb * k_steps / 2));
+  k_scatter<<<sm_count() * per_sm, kScatThreads, smem, st>>>(*e, A);
   int rc2 = launch_status();
   if (rc2 || e->vstim) return rc2;  // an external drive replaces the Philox draw
   const int64_t warps = (int64_t)nb * ((e->n + kDriveSpan - 1) / kDriveSpan);

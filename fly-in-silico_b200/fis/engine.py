@@ -373,9 +373,12 @@ class Core:
         _lib.check(rc, name)
         self.step += steps
 
-    def launches_per_block(self):
-        """Kernel launches of one block (scatter + update per trial group)."""
-        return 2 * (-(-self.batch // self.group))
+    def launches_per_block(self, rows=None):
+        """Kernel launches of one block: per trial group the scatter, the drive
+        (none under an external drive) and the update."""
+        nrows = self.batch if rows is None else max(1, min(int(rows), self.batch))
+        per_group = 3 if self.desc.vstim is None else 2
+        return per_group * (-(-nrows // self.group))
 
     # --- readouts -------------------------------------------------------------
 
