@@ -46,12 +46,56 @@ constexpr int kScatThreads = 256;
 constexpr int kScatWarps = kScatThreads / kWarp;
 constexpr int kMaxLists = 11264;  // prefix entries in dynamic shared memory (44 KB)
 
+// L2 eviction priorities (createpolicy, sm_80+).  The scratch ring is kept in
+// L2 between the scatter that fills it, the update that drains and clears it
+// and the next scatter (evict_last); the trial state streams through once
+// per block (evict_first), so it does not push the ring out.
+__device__ __forceinline__ uint64_t policy_keep() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;\n" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t policy_stream() {
+  uint64_t p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ float ld_hint(const float* a, uint64_t pol) {
+  float v;
+  asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;\n" : "=f"(v) : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ uint32_t ld_hint(const uint32_t* a, uint64_t pol) {
+  uint32_t v;
+  asm volatile("ld.global.L2::cache_hint.u32 %0, [%1], %2;\n" : "=r"(v) : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ uint32_t ld_hint(const uint8_t* a, uint64_t pol) {
+  uint32_t v;
+  asm volatile("ld.global.L2::cache_hint.u8 %0, [%1], %2;\n" : "=r"(v) : "l"(a), "l"(pol));
+  return v;
+}
+__device__ __forceinline__ void st_hint(float* a, float v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;\n" ::"l"(a), "f"(v), "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ void red_hint(uint32_t* a, uint32_t v, uint64_t pol) {
+  asm volatile("red.global.add.L2::cache_hint.u32 [%0], %1, %2;\n" ::"l"(a), "r"(v), "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ void red_hint(int32_t* a, int32_t v, uint64_t pol) {
+  asm volatile("red.global.add.L2::cache_hint.s32 [%0], %1, %2;\n" ::"l"(a), "r"(v), "l"(pol)
+               : "memory");
+}
+
 // Bulk asynchronous shared -> global copy (sm_90+ cp.async.bulk, the TMA
 // engine): both addresses 16-byte aligned, size a multiple of 16.
-__device__ __forceinline__ void bulk_store(void* gmem, const void* smem, unsigned bytes) {
+__device__ __forceinline__ void bulk_store(void* gmem, const void* smem, unsigned bytes,
+                                           uint64_t pol) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(gmem),
-               "r"(sa), "r"(bytes)
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group.L2::cache_hint [%0], [%1], %2, %3;\n" ::
+                   "l"(gmem),
+               "r"(sa), "r"(bytes), "l"(pol)
                : "memory");
 }
 __device__ __forceinline__ void bulk_commit() {
@@ -91,11 +135,11 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned by
 }
 // Bulk copy global -> shared, completing `bytes` transactions on `bar`.
 __device__ __forceinline__ void bulk_load(void* smem, const void* gmem, unsigned bytes,
-                                          uint64_t* bar) {
+                                          uint64_t* bar, uint64_t pol) {
   asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::
-          "r"(smem_addr(smem)),
-      "l"(gmem), "r"(bytes), "r"(smem_addr(bar))
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+      " [%0], [%1], %2, [%3], %4;\n" ::"r"(smem_addr(smem)),
+      "l"(gmem), "r"(bytes), "r"(smem_addr(bar)), "l"(pol)
       : "memory");
 }
 // Wait for phase `parity` of `bar`, giving up after `limit` polls (each poll
@@ -169,6 +213,7 @@ k_scatter(const fis_engine E, const ScatterArgs A) {
   const int B = E.batch;
   const int L = E.p.lag;
   const fis_clock ck = A.clk_given ? A.clk : *E.clock;
+  const uint64_t keep = policy_keep();  // the ring stays in L2 for the update
   const int64_t t0 = ck.step;
   const int64_t u_first = t0 + A.u_off;  // u_off is -lag: u_first = t0 mod lag
   const int64_t u_last = t0 - 1;
@@ -282,10 +327,10 @@ k_scatter(const fis_engine E, const ScatterArgs A) {
               // a signed count added to the low half carries into the high
               // half and back out, leaving it unchanged, while the biased
               // sums stay inside 0 .. 0xFFFF (exact below 2**15)
-              atomicAdd(reinterpret_cast<uint32_t*>(dst) + post,
-                        (uint32_t)edge_count(wv[c]) << shift);
+              red_hint(reinterpret_cast<uint32_t*>(dst) + post,
+                       (uint32_t)edge_count(wv[c]) << shift, keep);
             } else {
-              atomicAdd(dst + post, edge_count(wv[c]));
+              red_hint(dst + post, edge_count(wv[c]), keep);
             }
           }
         }
@@ -322,6 +367,7 @@ k_drive(const fis_engine E, const int b0, const int nb, const int K, const fis_c
   const fis_clock ck = clk_given ? clk : *E.clock;
   const int64_t t0 = ck.step;
   const int spans = (n + kDriveSpan - 1) / kDriveSpan;
+  const uint64_t stream = policy_stream();  // rates are read once per block
   const int64_t tasks = (int64_t)nb * spans;
   const int64_t nw = (int64_t)gridDim.x * (kDriveThreads / kWarp);
   for (int64_t task = (int64_t)blockIdx.x * (kDriveThreads / kWarp) + w; task < tasks;
@@ -338,7 +384,7 @@ k_drive(const fis_engine E, const int b0, const int nb, const int K, const fis_c
 #pragma unroll 4
     for (int c = 0; c < kDriveSpan / kWarp; ++c) {
       const int i = i0 + c * kWarp + lane;
-      const float p = i < n ? __fmul_rn(rates[i], E.p.prob_scale) : 0.f;
+      const float p = i < n ? __fmul_rn(ld_hint(rates + i, stream), E.p.prob_scale) : 0.f;
       const bool d = p > 0.f;
       const unsigned m = __ballot_sync(0xFFFFFFFFu, d);
       if (d) {
@@ -617,6 +663,8 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
   const int64_t toff = kHalf ? ((int64_t)pp * NR + tile * kTile) * 2
                              : (int64_t)(2 * pp) * NR + tile * kTile;
   const int copies = kHalf ? K : K * nt;  // 1 KB lines to stage
+  const uint64_t keep = policy_keep();      // the scratch ring
+  const uint64_t stream = policy_stream();  // the trial state
 
   // Stage the tile's K slots: warp 0 sets up the barrier and issues the bulk
   // copies (TMA), all completing on that barrier.
@@ -633,7 +681,7 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
         const int64_t off = (int64_t)k * sstride + toff + (int64_t)t * NR;
         const void* src = kHalf ? (const void*)(reinterpret_cast<const uint16_t*>(ring) + off)
                                 : (const void*)(ring + off);
-        bulk_load(&sring[k][t * kTile], src, kTile * 4u, &sbar);
+        bulk_load(&sring[k][t * kTile], src, kTile * 4u, &sbar, keep);
       }
     }
   }
@@ -654,12 +702,12 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
     fl[t] = dm[t] = 0;
     rate[t] = vv[t] = gg[t] = rr[t] = 0.f;
     if (valid && t < nt) {
-      vv[t] = E.v[sidx[t]];
-      gg[t] = E.g[sidx[t]];
-      rr[t] = E.refrac[sidx[t]];
-      fl[t] = E.flags[sidx[t]];
-      rate[t] = E.rates[sidx[t]];
-      if (!kTape) dm[t] = E.kicks[sidx[t]];
+      vv[t] = ld_hint(E.v + sidx[t], stream);
+      gg[t] = ld_hint(E.g + sidx[t], stream);
+      rr[t] = ld_hint(E.refrac + sidx[t], stream);
+      fl[t] = ld_hint(E.flags + sidx[t], stream);
+      rate[t] = ld_hint(E.rates + sidx[t], stream);
+      if (!kTape) dm[t] = ld_hint(E.kicks + sidx[t], stream);
     }
   }
   __syncthreads();  // the staging barrier exists before anyone waits on it
@@ -717,8 +765,8 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
     for (int c = threadIdx.x; c < copies; c += kWarp) {
       const int k = kHalf ? c : c / nt, t = kHalf ? 0 : c - k * nt;
       const int64_t off = (int64_t)k * sstride + toff + (int64_t)t * NR;
-      if (kHalf) bulk_store(reinterpret_cast<uint16_t*>(ring) + off, szero, kTile * 4u);
-      else bulk_store(ring + off, szero, kTile * 4u);
+      if (kHalf) bulk_store(reinterpret_cast<uint16_t*>(ring) + off, szero, kTile * 4u, keep);
+      else bulk_store(ring + off, szero, kTile * 4u, keep);
     }
     bulk_commit();
   }
@@ -821,9 +869,9 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
       bitrow[t][sl] = sbal[t][wib][lane];
     }
     if (valid) {
-      E.v[sidx[t]] = ov[t];
-      E.g[sidx[t]] = og[t];
-      E.refrac[sidx[t]] = orr[t];
+      st_hint(E.v + sidx[t], ov[t], stream);
+      st_hint(E.g + sidx[t], og[t], stream);
+      st_hint(E.refrac + sidx[t], orr[t], stream);
       if (spikes_out) spikes_out[sidx[t]] = (okeep[t] == 0.f) ? 1.f : 0.f;
     }
     // Spike lists and recording for the (rare) steps this neuron fired.
