@@ -710,8 +710,14 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
       if (!kTape) dm[t] = ld_hint(E.kicks + sidx[t], stream);
     }
   }
+  // this neuron's chunk count, for the spike lists of the epilogue
+  const int nch = valid ? (int)E.nchunks[i] : 0;
   __syncthreads();  // the staging barrier exists before anyone waits on it
   const int64_t t0 = ck.step;
+  int32_t* recp[2];  // the trials' recording buffers, read long before the epilogue
+#pragma unroll
+  for (int t = 0; t < 2; ++t)
+    recp[t] = (tr[t].rec >= 0 && tr[t].rec < E.n_recs) ? E.recs[tr[t].rec] : nullptr;
   const int slot0 = ck.slot;  // ring-of-lists slot of step t0
   int ka[2], kb[2];
   bool runs[2];
@@ -879,7 +885,6 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
     if (fired) {
       const int B = E.batch;
       const bool out_on = !(fl[t] & (FIS_FL_OUT_OFF | FIS_FL_SILENCED));
-      const int nch = E.nchunks[i];
       const int slot20 = ck.slot2;
       const int64_t own0 = t0 - tr[t].start;
       while (fired) {
@@ -897,7 +902,7 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
           const int64_t own = own0 + k;
           const int64_t bin = own < 0x7FFFFFFF ? (int64_t)((int)own / tr[t].bin_steps)
                                                 : own / tr[t].bin_steps;
-          if (bin < tr[t].n_bins) atomicAdd(E.recs[tr[t].rec] + bin * n + i, 1);
+          if (bin < tr[t].n_bins) red_hint(recp[t] + bin * n + i, 1, stream);
         }
       }
     }
