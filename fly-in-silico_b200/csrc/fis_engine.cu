@@ -707,7 +707,7 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
       rr[t] = ld_hint(E.refrac + sidx[t], stream);
       fl[t] = ld_hint(E.flags + sidx[t], stream);
       rate[t] = ld_hint(E.rates + sidx[t], stream);
-      if (!kTape) dm[t] = ld_hint(E.kicks + sidx[t], stream);
+      if (!kTape && K > 1) dm[t] = ld_hint(E.kicks + sidx[t], stream);
     }
   }
   // this neuron's chunk count, for the spike lists of the epilogue
@@ -731,7 +731,20 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
     runs[t] = t < nt && ka[t] < kb[t];  // uniform across the CTA
     if (!runs[t]) fl[t] = 0, rate[t] = vv[t] = gg[t] = rr[t] = 0.f;
     // kick steps were computed by phase A for neurons with a positive rate
-    if (!(runs[t] && __fmul_rn(rate[t], E.p.prob_scale) > 0.f)) dm[t] = 0u;
+    // (a one-step block draws its word here: word own % 4 of Philox4x32-10
+    // at counter (i, own / 4, trial lane), as k_drive does)
+    const float prob = __fmul_rn(rate[t], E.p.prob_scale);
+    if (!(runs[t] && prob > 0.f)) {
+      dm[t] = 0u;
+    } else if (!kTape && K == 1 && valid) {
+      const int64_t own = t0 - tr[t].start;
+      const uint64_t quad = (uint64_t)(own >> 2);
+      const Philox4 r4 = philox4((uint32_t)i, (uint32_t)quad, (uint32_t)(quad >> 32), tr[t].stream,
+                                 (uint32_t)tr[t].seed, (uint32_t)(tr[t].seed >> 32));
+      const int w = (int)(own & 3);  // selected without indexing (stays in registers)
+      const uint32_t x = w & 2 ? (w & 1 ? r4.x[3] : r4.x[2]) : (w & 1 ? r4.x[1] : r4.x[0]);
+      dm[t] = __fmul_rn((float)(x >> 8), 0x1p-24f) < prob ? 1u : 0u;
+    }
     drv_any = drv_any || (valid && runs[t] && __fmul_rn(rate[t], E.p.prob_scale) > 0.f);
     bitrow[t] = E.bits + ((int64_t)(b0 + 2 * pp + (t < nt ? t : 0)) * Wd + (i >> 5)) * L;
     s_prev[t] = false;
@@ -1121,7 +1134,9 @@ int scatter_block(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, 
   const int per_sm = std::min(8, std::max(1, nb * k_steps / 2));
   k_scatter<<<sm_count() * per_sm, kScatThreads, smem, st>>>(*e, A);
   int rc2 = launch_status();
-  if (rc2 || e->vstim) return rc2;  // an external drive replaces the Philox draw
+  // An external drive replaces the Philox draw; a one-step block draws its one
+  // Philox word per driven neuron inside the update (no launch for so little).
+  if (rc2 || e->vstim || k_steps == 1) return rc2;
   const int64_t warps = (int64_t)nb * ((e->n + kDriveSpan - 1) / kDriveSpan);
   const int64_t cap = (int64_t)sm_count() * 8;
   const int64_t blocks = (warps + kDriveThreads / kWarp - 1) / (kDriveThreads / kWarp);
