@@ -344,11 +344,13 @@ def main():
     units_rank = args.trials * conn.n * args.sim_steps
     value = world * units_rank * args.steps / (ms / 1000.0)
 
-    # end to end through the public API: host specs in, host counts out
+    # end to end through the public API: host specs in, host counts out; one
+    # untimed run first warms the pinned staging buffers and the path
+    batch.run(specs)
     barrier()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        batch.run(specs)
+    for _ in batch.run_many(specs for _ in range(args.steps)):
+        pass
     barrier()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     e2e = world * units_rank * args.steps / e2e_s

@@ -129,15 +129,7 @@ class Batch:
         self._recs = {}                          # index -> int32 [n_bins][N]
         self._rec_refs = {}                      # index -> trials recording into it
         self._slot_rec = [None] * self.capacity  # slot -> index
-        self._pinned = {}
         self._dummy_rec = None
-
-    def _staging(self, name, shape, dtype):
-        buf = self._pinned.get(name)
-        if buf is None or buf.shape != shape:
-            buf = torch.empty(shape, dtype=dtype, pin_memory=True)
-            self._pinned[name] = buf
-        return buf
 
     # --- recording registry ---------------------------------------------------
 
@@ -175,24 +167,16 @@ class Batch:
 
     # --- trials -------------------------------------------------------------------
 
-    def load(self, slots, specs, start=None, rec=None):
-        """Place ``specs`` into ``slots`` starting at global step ``start``.
+    def _rows_host(self, specs, slots):
+        """The sparse rows of ``specs`` in ``slots``, packed into one pinned buffer.
 
-        The trials' non-zero flags and rates travel sparse (positions and
-        values, one pinned copy) and are laid into the zeroed rows on the
-        device; state is reset to the reference's initial values.  ``rec``: a
-        shared recording buffer for all these trials; by default each trial
-        gets one of its own (views of one buffer when their bin counts agree).
+        Layout: int64 flag positions, int64 rate positions (8-byte aligned),
+        float32 rates, uint8 flag bits.  The buffer comes from torch's caching
+        host allocator, which keeps it until the copy that reads it has run.
         """
-        c = self.core
-        slots = list(slots)
-        k = len(slots)
-        start = c.step if start is None else int(start)
         fa, fb, ra, rv = sparse_rows(specs, self.n, slots)
-        # one pinned staging buffer: int64 positions first (8-byte aligned), then
-        # float32 rates, then uint8 flag bits
         nbytes = 8 * (fa.size + ra.size) + 4 * rv.size + fb.size
-        pin = self._staging("rows", (max(8, -(-nbytes // 8) * 8),), torch.uint8)
+        pin = torch.empty(max(8, -(-nbytes // 8) * 8), dtype=torch.uint8, pin_memory=True)
         host = pin.numpy()
         o1, o2 = 8 * fa.size, 8 * (fa.size + ra.size)
         o3 = o2 + 4 * rv.size
@@ -200,6 +184,23 @@ class Batch:
         host[o1:o2].view(np.int64)[:] = ra
         host[o2:o3].view(np.float32)[:] = rv
         host[o3:o3 + fb.size] = fb
+        return pin, nbytes, (o1, o2, o3, fa.size, ra.size, fb.size)
+
+    def load(self, slots, specs, start=None, rec=None, staged=None):
+        """Place ``specs`` into ``slots`` starting at global step ``start``.
+
+        The trials' non-zero flags and rates travel sparse (positions and
+        values, one pinned copy) and are laid into the zeroed rows on the
+        device; state is reset to the reference's initial values.  ``rec``: a
+        shared recording buffer for all these trials; by default each trial
+        gets one of its own (views of one buffer when their bin counts agree).
+        ``staged``: the rows already packed by ``_rows_host`` for these slots.
+        """
+        c = self.core
+        slots = list(slots)
+        k = len(slots)
+        start = c.step if start is None else int(start)
+        pin, nbytes, (o1, o2, o3, nfa, nra, nfb) = staged or self._rows_host(specs, slots)
         dev = pin[:nbytes].to(c.device, non_blocking=True)
         self.last_h2d_bytes = nbytes
         idx = torch.as_tensor(slots, dtype=torch.long, device=c.device)
@@ -207,9 +208,9 @@ class Batch:
         rows = slice(slots[0], slots[0] + k) if contiguous else idx
         c.flags[rows] = 0
         c.rates[rows] = 0.0
-        if fa.size:
-            c.flags.view(-1)[dev[:o1].view(torch.int64)] = dev[o3:o3 + fb.size]
-        if ra.size:
+        if nfa:
+            c.flags.view(-1)[dev[:o1].view(torch.int64)] = dev[o3:o3 + nfb]
+        if nra:
             c.rates.view(-1)[dev[o1:o2].view(torch.int64)] = dev[o2:o3].view(torch.float32)
         for b in slots:
             if self._slot_rec[b] is not None:
@@ -243,27 +244,30 @@ class Batch:
         c.mark_trials()
         c.reset_slots(rows)
 
-    def run(self, specs, timer=None):
-        """Run ``specs`` (at most ``capacity``) to completion; host counts per trial.
-
-        Trials are placed longest first, so the running ones always fill the
-        lowest slots: once every trial of the last trial group has ended, that
-        group is no longer launched.  ``slots_of_run[j]`` is the slot that ran
-        ``specs[j]``.  Returns int32 [len(specs)][N] spike counts summed over
-        each trial's bins, in the order of ``specs``, copied to the host.
-        """
-        c = self.core
+    def _plan(self, specs):
+        """Host side of a run: placement (longest first) and the packed rows."""
         k = len(specs)
         if k > self.capacity:
             raise ValueError("%d trials for %d slots" % (k, self.capacity))
         order = sorted(range(k), key=lambda j: -int(specs[j].steps))
-        self.slots_of_run = [0] * k
+        slots_of_run = [0] * k
         for slot, j in enumerate(order):
-            self.slots_of_run[j] = slot
+            slots_of_run[j] = slot
+        placed = [specs[j] for j in order]
+        return {"specs": placed, "slots_of_run": slots_of_run,
+                "staged": self._rows_host(placed, list(range(k)))}
+
+    def _launch(self, plan, timer=None):
+        """Device side of a run, all enqueued: load, advance, per-trial counts
+        into a pinned host buffer.  Returns the handle ``_finish`` waits on."""
+        c = self.core
+        placed = plan["specs"]
+        k = len(placed)
+        self.slots_of_run = plan["slots_of_run"]
         for b in range(k, self.capacity):   # idle slots do nothing
             c.trials[b].start = c.trials[b].end = 0
-        self.load(range(k), [specs[j] for j in order])
-        dur = [int(specs[j].steps) for j in order]
+        self.load(range(k), placed, staged=plan["staged"])
+        dur = [int(s.steps) for s in placed]
         G, K = c.group, c.max_block
         t, total = 0, dur[0] if dur else 0
         while t < total:
@@ -273,7 +277,7 @@ class Batch:
             nxt = min(total, t + -(-(nxt - t) // K) * K)  # whole blocks
             c.advance(nxt - t, timer=timer, rows=rows)
             t = nxt
-        out = self._staging("counts", (k, self.n), torch.int32)
+        out = torch.empty((k, self.n), dtype=torch.int32, pin_memory=True)
         if self.last_recording is not None:  # [k][n_bins][N], trials in slot order
             sums = self.last_recording.sum(1, dtype=torch.int32)
             pos = torch.as_tensor(self.slots_of_run, dtype=torch.long, device=c.device)
@@ -283,9 +287,43 @@ class Batch:
                                for j in range(k)])
         out.copy_(dev, non_blocking=True)
         self.last_d2h_bytes = out.numel() * out.element_size()
-        torch.cuda.current_stream(c.device).synchronize()
-        c.check_errors()
+        done = torch.cuda.Event()
+        done.record(torch.cuda.current_stream(c.device))
+        return out, done
+
+    def _finish(self, handle):
+        out, done = handle
+        done.synchronize()
+        self.core.check_errors()
         return out.numpy().copy()
+
+    def run(self, specs, timer=None):
+        """Run ``specs`` (at most ``capacity``) to completion; host counts per trial.
+
+        Trials are placed longest first, so the running ones always fill the
+        lowest slots: once every trial of the last trial group has ended, that
+        group is no longer launched.  ``slots_of_run[j]`` is the slot that ran
+        ``specs[j]``.  Returns int32 [len(specs)][N] spike counts summed over
+        each trial's bins, in the order of ``specs``, copied to the host.
+        """
+        return self._finish(self._launch(self._plan(specs), timer=timer))
+
+    def run_many(self, spec_lists):
+        """``run`` over several batches, one after another on the device.
+
+        The host packs the next batch's rows while the device runs the
+        current one, so the device does not wait for the host between
+        batches.  Yields each batch's counts (as ``run`` returns them) as it
+        completes.
+        """
+        pending = None
+        for specs in spec_lists:
+            plan = self._plan(specs)          # overlaps the previous batch's run
+            if pending is not None:
+                yield self._finish(pending)
+            pending = self._launch(plan)
+        if pending is not None:
+            yield self._finish(pending)
 
 
 def random_specs(n, count, seed, steps, stim_range=(500, 5000), rate_range=(50.0, 300.0),

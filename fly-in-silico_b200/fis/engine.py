@@ -254,8 +254,12 @@ class Core:
 
     def _sync_trials(self):
         if self._trials_dirty:
-            host = torch.frombuffer(bytearray(bytes(self.trials)), dtype=torch.uint8)
-            self.trials_dev.copy_(host)
+            # a fresh pinned buffer from torch's caching host allocator, which
+            # holds it until the asynchronous copy has run: the host does not
+            # wait for the stream
+            host = torch.empty(ctypes.sizeof(self.trials), dtype=torch.uint8, pin_memory=True)
+            ctypes.memmove(host.data_ptr(), ctypes.addressof(self.trials), ctypes.sizeof(self.trials))
+            self.trials_dev.copy_(host, non_blocking=True)
             self._trials_dirty = False
 
     def mark_trials(self):

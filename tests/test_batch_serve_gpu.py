@@ -165,3 +165,16 @@ def test_last_step_raster_mode_keeps_state_and_last_spikes():
                 core.spikes_at(core.step - 2)
     for a, b in zip(got[0], got[1]):
         assert np.array_equal(a, b)
+
+
+def test_run_many_equals_run():
+    """The pipelined run_many gives each batch exactly what run gives it."""
+    from fis.batch import Batch
+
+    c = conn()
+    batches = [specs(91, 3, (40, 120)), specs(92, 4, 60), specs(93, 2, (20, 90))]
+    want = [Batch(c, 4, group=2).run(sp) for sp in batches]
+    got = list(Batch(c, 4, group=2).run_many(batches))
+    assert len(got) == len(want)
+    for a, b in zip(got, want):
+        assert np.array_equal(a, b)
