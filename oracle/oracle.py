@@ -181,8 +181,11 @@ class Oracle:
 
     def __del__(self):
         h = getattr(self, "_h", None)
-        if h:
-            lib().oracle_destroy(h)
+        if h and lib is not None:  # module globals may be gone at interpreter exit
+            try:
+                lib().oracle_destroy(h)
+            except TypeError:
+                pass
             self._h = None
 
     def set_masks(self, fire=None, out=None, inc=None, hold=None, v_clamp=None,
