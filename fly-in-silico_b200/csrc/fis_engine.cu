@@ -206,9 +206,9 @@ struct ScatterArgs {
 // The value that marks an empty pair of biased uint16 ring elements.
 constexpr uint32_t kEmptyPair = 0x80008000u;
 
-__global__ void __launch_bounds__(kScatThreads)
-k_scatter(const fis_engine E, const ScatterArgs A) {
-  extern __shared__ int32_t pre_sum[];
+// The scatter's work for CTA `bid` of `nblk`; `pre_sum` holds (K+1)*nb+1 ints.
+__device__ __forceinline__ void scatter_body(const fis_engine& E, const ScatterArgs& A,
+                                             const int bid, const int nblk, int32_t* pre_sum) {
   const int n = E.n;
   const int B = E.batch;
   const int L = E.p.lag;
@@ -241,30 +241,37 @@ k_scatter(const fis_engine E, const ScatterArgs A) {
       pre_sum[j] = len;  // provisional
       acc += len;
     }
-    __shared__ int32_t part[kScatThreads];
-    part[threadIdx.x] = acc;
-    __syncthreads();
-    // inclusive scan of the per-thread partial sums (Hillis-Steele)
-    for (int off = 1; off < kScatThreads; off <<= 1) {
-      const int32_t x = threadIdx.x >= off ? part[threadIdx.x - off] : 0;
-      __syncthreads();
-      part[threadIdx.x] += x;
-      __syncthreads();
+    // exclusive scan of the per-thread partial sums: within each warp by
+    // shuffles, then over the eight warp totals
+    __shared__ int32_t wsum[kScatWarps];
+    const int ln = threadIdx.x & (kWarp - 1), wp = threadIdx.x / kWarp;
+    int32_t inc = acc;
+#pragma unroll
+    for (int off = 1; off < kWarp; off <<= 1) {
+      const int32_t x = __shfl_up_sync(0xFFFFFFFFu, inc, off);
+      if (ln >= off) inc += x;
     }
-    int32_t run = threadIdx.x ? part[threadIdx.x - 1] : 0;
+    if (ln == kWarp - 1) wsum[wp] = inc;
+    __syncthreads();
+    int32_t before = 0, all = 0;
+#pragma unroll
+    for (int w = 0; w < kScatWarps; ++w) {
+      before += w < wp ? wsum[w] : 0;
+      all += wsum[w];
+    }
+    int32_t run = before + inc - acc;
     for (int j = j0; j < j0 + per && j < nlists; ++j) {
       const int32_t len = pre_sum[j];
       pre_sum[j] = run;
       run += len;
     }
-    __syncthreads();
-    if (threadIdx.x == 0) pre_sum[nlists] = part[kScatThreads - 1];
+    if (threadIdx.x == 0) pre_sum[nlists] = all;
     __syncthreads();
   }
   const int32_t total = pre_sum[nlists];
 
   // Lists that the following update phase will write start empty.
-  if (blockIdx.x == 0) {
+  if (bid == 0) {
     for (int j = threadIdx.x; j < A.zero_next * A.nb; j += blockDim.x) {
       const int kk = j / A.nb, bl = j - kk * A.nb;
       E.list_len[wrap(ck.slot2 + kk, 2 * L) * B + A.b0 + bl] = 0;
@@ -277,7 +284,7 @@ k_scatter(const fis_engine E, const ScatterArgs A) {
   // [slot][pair][trial_stride] 32-bit words, trial 2p in the low half of each
   // word and trial 2p + 1 in the high half.
   const int64_t slot_stride = (int64_t)(A.half ? (A.nb + 1) >> 1 : A.nb) * A.trial_stride;
-  for (int32_t w = blockIdx.x * kScatWarps + warp; w < total; w += gridDim.x * kScatWarps) {
+  for (int32_t w = bid * kScatWarps + warp; w < total; w += nblk * kScatWarps) {
     // list holding work item w: largest j with pre_sum[j] <= w
     int lo = 0, hi = nlists - 1;
     while (lo < hi) {
@@ -355,9 +362,9 @@ k_scatter(const fis_engine E, const ScatterArgs A) {
 constexpr int kDriveThreads = 256;
 constexpr int kDriveSpan = 256;  // neurons per warp task
 
-__global__ void __launch_bounds__(kDriveThreads)
-k_drive(const fis_engine E, const int b0, const int nb, const int K, const fis_clock clk,
-        const int clk_given) {
+__device__ __forceinline__ void drive_body(const fis_engine& E, const int b0, const int nb,
+                                           const int K, const fis_clock& clk,
+                                           const int clk_given, const int bid, const int nblk) {
   __shared__ uint16_t slist[kDriveThreads / kWarp][kDriveSpan];  // offset in the span
   __shared__ float sprob[kDriveThreads / kWarp][kDriveSpan];
   __shared__ uint32_t sbits[kDriveThreads / kWarp][kDriveSpan];
@@ -369,8 +376,8 @@ k_drive(const fis_engine E, const int b0, const int nb, const int K, const fis_c
   const int spans = (n + kDriveSpan - 1) / kDriveSpan;
   const uint64_t stream = policy_stream();  // rates are read once per block
   const int64_t tasks = (int64_t)nb * spans;
-  const int64_t nw = (int64_t)gridDim.x * (kDriveThreads / kWarp);
-  for (int64_t task = (int64_t)blockIdx.x * (kDriveThreads / kWarp) + w; task < tasks;
+  const int64_t nw = (int64_t)nblk * (kDriveThreads / kWarp);
+  for (int64_t task = (int64_t)bid * (kDriveThreads / kWarp) + w; task < tasks;
        task += nw) {
     const int bl = (int)(task / spans);
     const int i0 = (int)(task - (int64_t)bl * spans) * kDriveSpan;
@@ -422,6 +429,27 @@ k_drive(const fis_engine E, const int b0, const int nb, const int K, const fis_c
     for (int j = lane; j < cnt; j += kWarp) kicks[slist[w][j]] = sbits[w][j];
     __syncwarp();  // the lists are reused by the warp's next task
   }
+}
+
+// The scatter alone (the delay-ring readout uses it).
+__global__ void __launch_bounds__(kScatThreads)
+k_scatter(const fis_engine E, const ScatterArgs A) {
+  extern __shared__ int32_t pre_sum[];
+  scatter_body(E, A, blockIdx.x, gridDim.x, pre_sum);
+}
+
+// Phase A of a block as one grid: CTAs [0, scat) scatter, the rest draw the
+// Poisson drive.  Both are latency-bound; in one grid their CTAs share the
+// SMs and fill each other's waits, and the block needs one launch less.
+static_assert(kScatThreads == kDriveThreads, "one block size for both roles");
+__global__ void __launch_bounds__(kScatThreads)
+k_phase_a(const fis_engine E, const ScatterArgs A, const int scat) {
+  extern __shared__ int32_t pre_sum[];
+  if ((int)blockIdx.x < scat)
+    scatter_body(E, A, blockIdx.x, scat, pre_sum);
+  else
+    drive_body(E, A.b0, A.nb, A.nsrc, A.clk, A.clk_given, blockIdx.x - scat,
+               gridDim.x - scat);
 }
 
 // ---------------------------------------------------------------------------
@@ -1132,16 +1160,19 @@ int scatter_block(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, 
   // up to 8 CTAs per SM; fewer for small blocks (one trial, one step), where
   // the spikes of a step fill one pass of a CTA per SM
   const int per_sm = std::min(8, std::max(1, nb * k_steps / 2));
-  k_scatter<<<sm_count() * per_sm, kScatThreads, smem, st>>>(*e, A);
-  int rc2 = launch_status();
   // An external drive replaces the Philox draw; a one-step block draws its one
-  // Philox word per driven neuron inside the update (no launch for so little).
-  if (rc2 || e->vstim || k_steps == 1) return rc2;
-  const int64_t warps = (int64_t)nb * ((e->n + kDriveSpan - 1) / kDriveSpan);
-  const int64_t cap = (int64_t)sm_count() * 8;
-  const int64_t blocks = (warps + kDriveThreads / kWarp - 1) / (kDriveThreads / kWarp);
-  k_drive<<<(int)(blocks < cap ? blocks : cap), kDriveThreads, 0, st>>>(
-      *e, b0, nb, k_steps, A.clk, A.clk_given);
+  // Philox word per driven neuron inside the update (no CTAs for so little).
+  // With a drive, both roles fit one wave (5 CTAs of this kernel per SM): up
+  // to 3 scattering and 2 drawing per SM.
+  int drive = 0;
+  if (!e->vstim && k_steps > 1) {
+    const int64_t warps = (int64_t)nb * ((e->n + kDriveSpan - 1) / kDriveSpan);
+    const int64_t cap = (int64_t)sm_count() * 2;
+    const int64_t blocks = (warps + kDriveThreads / kWarp - 1) / (kDriveThreads / kWarp);
+    drive = (int)(blocks < cap ? blocks : cap);
+  }
+  const int scat = sm_count() * (drive ? std::min(per_sm, 3) : per_sm);
+  k_phase_a<<<scat + drive, kScatThreads, smem, st>>>(*e, A, scat);
   return launch_status();
 }
 
