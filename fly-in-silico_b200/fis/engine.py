@@ -378,11 +378,10 @@ class Core:
         self.step += steps
 
     def launches_per_block(self, rows=None):
-        """Kernel launches of one block: per trial group the scatter, the drive
-        (none under an external drive) and the update."""
+        """Kernel launches of one block: per trial group the phase-A grid
+        (scatter and Poisson drive) and the update."""
         nrows = self.batch if rows is None else max(1, min(int(rows), self.batch))
-        per_group = 3 if self.desc.vstim is None else 2
-        return per_group * (-(-nrows // self.group))
+        return 2 * (-(-nrows // self.group))
 
     # --- readouts -------------------------------------------------------------
 
