@@ -760,7 +760,7 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
     if (!runs[t]) fl[t] = 0, rate[t] = vv[t] = gg[t] = rr[t] = 0.f;
     // kick steps were computed by phase A for neurons with a positive rate
     // (a one-step block draws its word here: word own % 4 of Philox4x32-10
-    // at counter (i, own / 4, trial lane), as k_drive does)
+    // at counter (i, own / 4, trial lane), as the phase-A drive does)
     const float prob = __fmul_rn(rate[t], E.p.prob_scale);
     if (!(runs[t] && prob > 0.f)) {
       dm[t] = 0u;
