@@ -534,6 +534,15 @@ __device__ __forceinline__ f2 subp(const Consts& C, f2 c, f2 p) { return fma2(p,
 // +0, which can change only the sign of a zero sum -- and the conductance
 // reset below, gn - gn * spike, turns either zero into +0.  So the stored
 // state is the same bits, for two multiplies fewer per step.
+//
+// kStim: add the step's external drive `vstim`.  kHold: apply the hold.  For
+// a warp with no driven and no held lane both are identities once v is not
+// -0 (v + 0 and v * 1 + 0 leave any other v unchanged), and v never becomes
+// -0 inside the loop: x + y is -0 only when both are -0, so neither the
+// membrane update v + p nor the reset v - d * spike (d = v - v_reset, x - x
+// = +0) turns a v that is not -0 into -0.  The loop adds +0 once before its
+// first step (the reference's own v + 0) and then leaves both out.
+template <bool kStim = true, bool kHold = true>
 __device__ __forceinline__ void lif_step2(Pair& s, const Consts& C, int32_t c0, int32_t c1,
                                           f2 vstim, bool& f0, bool& f1, f2& sp) {
   // refractory counter and gate (sim.py:921-923); r is the previous step's
@@ -546,12 +555,12 @@ __device__ __forceinline__ void lif_step2(Pair& s, const Consts& C, int32_t c0, 
   const f2 delayed = mul2(C.w, pk2(__int2float_rn(g0), __int2float_rn(g1)));
   const f2 gn = addp(C, mul2(s.g, C.a_syn), delayed);
   // membrane with the previous conductance (sim.py:936-938)
-  f2 v = add2(s.v, vstim);
+  f2 v = kStim ? add2(s.v, vstim) : s.v;
   v = addp(C, mul2(C.a_mem, sub2(s.g, sub2(v, C.v_rest))), v);
   // hold, threshold, reset (sim.py:943-952).  spikes = (v > v_th) * m_fire
   // with m_fire in {0, 1} is +0 or 1; comparing against +inf where m_fire is
   // 0 gives the same bits (a finite v never exceeds +inf) without the multiply.
-  v = addp(C, mul2(v, s.m_hold), s.v_hold);
+  if (kHold) v = addp(C, mul2(v, s.m_hold), s.v_hold);
   float v0, v1;
   up2(v, v0, v1);
   f0 = v0 > s.vth0;
@@ -597,7 +606,8 @@ __device__ __forceinline__ void staged2(const Staged2& s, int k, int32_t& c0, in
 // step.  `kRaster`: store every step's raster words (else the caller keeps
 // only the last step's).  Returns the fired steps of each trial as bits, the
 // last step in bit 0 (exact in float).
-template <bool kTape, bool kDrive, bool kHalf, bool kPartial, bool kRaster = true>
+template <bool kTape, bool kDrive, bool kHalf, bool kPartial, bool kRaster = true,
+          bool kHold = true>
 __device__ __forceinline__ f2 step_loop2(Pair& st, const Consts& C, const fis_engine& E, int K,
                                          int ka0, int kb0, int ka1, int kb1, uint32_t dm0,
                                          uint32_t dm1, const Staged2& in, uint32_t* sbal0,
@@ -608,6 +618,9 @@ __device__ __forceinline__ f2 step_loop2(Pair& st, const Consts& C, const fis_en
   // 20 bits (bookkeeping, not model state, so the fused multiply-add is fine)
   f2 nspk = pk2(0.f, 0.f);
   const f2 two = pk2(2.f, 2.f);
+  // no external drive in this warp: its per-step v + 0 is done once here
+  constexpr bool kStim = kTape || kDrive || kPartial;
+  if (!kStim) st.v = add2(st.v, pk2(0.f, 0.f));
   // Lanes past the last neuron run the same arithmetic on inert values (never
   // above an infinite threshold) and store nothing.  Every lane stores the
   // warp's ballot word (the same value to the same address), so the store
@@ -642,7 +655,7 @@ __device__ __forceinline__ f2 step_loop2(Pair& st, const Consts& C, const fis_en
       f1 = f1 && a1;
       sp = pk2(f0 ? 1.f : 0.f, f1 ? 1.f : 0.f);
     } else {
-      lif_step2(st, C, c0, c1, vstim, f0, f1, sp);
+      lif_step2<kStim, kHold || kPartial>(st, C, c0, c1, vstim, f0, f1, sp);
     }
     if (kRaster) {
       sbal0[k] = __ballot_sync(0xFFFFFFFFu, f0);
@@ -860,6 +873,7 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
   // block needs the per-step commit of the partial loop.
   const bool full = (!runs[0] || (ka[0] == 0 && kb[0] == K)) &&
                     (!runs[1] || (ka[1] == 0 && kb[1] == K));
+  const bool hold_any = __any_sync(0xFFFFFFFFu, ((fl[0] | fl[1]) & FIS_FL_HOLD) != 0);
   uint32_t* sb0 = sbal[0][wib];
   uint32_t* sb1 = sbal[1][wib];
   f2 nspk;
@@ -878,12 +892,18 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
   else if (E.raster)
     nspk = step_loop2<false, false, kHalf, false>(st, C, E, K, 0, K, 0, K, 0u, 0u, in, sb0, sb1,
                                                  sidx[0], sidx[1], valid);
-  else if (warp_driven)
+  else if (hold_any && warp_driven)
     nspk = step_loop2<false, true, kHalf, false, false>(st, C, E, K, 0, K, 0, K, dm[0], dm[1], in,
                                                        sb0, sb1, sidx[0], sidx[1], valid);
-  else
+  else if (hold_any)
     nspk = step_loop2<false, false, kHalf, false, false>(st, C, E, K, 0, K, 0, K, 0u, 0u, in,
                                                         sb0, sb1, sidx[0], sidx[1], valid);
+  else if (warp_driven)  // no held lane: the hold is left out (see lif_step2)
+    nspk = step_loop2<false, true, kHalf, false, false, false>(
+        st, C, E, K, 0, K, 0, K, dm[0], dm[1], in, sb0, sb1, sidx[0], sidx[1], valid);
+  else
+    nspk = step_loop2<false, false, kHalf, false, false, false>(
+        st, C, E, K, 0, K, 0, K, 0u, 0u, in, sb0, sb1, sidx[0], sidx[1], valid);
   // Without the full raster only the last step's words are kept (the next
   // block reads them for the refractory reset); the partial and tape loops
   // always store every step.
