@@ -1182,16 +1182,21 @@ int scatter_block(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, 
   const int per_sm = std::min(8, std::max(1, nb * k_steps / 2));
   // An external drive replaces the Philox draw; a one-step block draws its one
   // Philox word per driven neuron inside the update (no CTAs for so little).
-  // With a drive, both roles fit one wave (5 CTAs of this kernel per SM): up
-  // to 3 scattering and 2 drawing per SM.
+  // With a drive, the grid is sized for the overlapped pipeline, where it
+  // runs beside the previous group's update: every resident phase-A CTA holds
+  // register-file room that an update CTA would use, so the grid is the
+  // smallest that still ends within an update.  Up to 1.5 scattering and 3
+  // drawing CTAs per SM (4.5 per SM, one wave at 5 per SM) measured best on
+  // the full connectome for trial groups of 16 to 64.
   int drive = 0;
   if (!e->vstim && k_steps > 1) {
     const int64_t warps = (int64_t)nb * ((e->n + kDriveSpan - 1) / kDriveSpan);
-    const int64_t cap = (int64_t)sm_count() * 2;
+    const int64_t cap = (int64_t)sm_count() * 3;
     const int64_t blocks = (warps + kDriveThreads / kWarp - 1) / (kDriveThreads / kWarp);
     drive = (int)(blocks < cap ? blocks : cap);
   }
-  const int scat = sm_count() * (drive ? std::min(per_sm, 3) : per_sm);
+  const int scat = drive ? std::max(sm_count(), sm_count() * std::min(per_sm, 3) / 2)
+                         : sm_count() * per_sm;
   k_phase_a<<<scat + drive, kScatThreads, smem, st>>>(*e, A, scat);
   return launch_status();
 }
