@@ -203,6 +203,66 @@ def test_ev_spmv_dropin_exact():
     assert np.array_equal(out, want.astype(np.float32))
 
 
+def _bits(a):
+    return np.ascontiguousarray(a).view(np.uint32)
+
+
+@pytest.mark.parametrize("ring", ["int16", "int32"])
+def test_injected_refractory_counts_match_oracle(ring):
+    """Refractory counts written into the state continue as the oracle's, bit
+    for bit and signed zeros included (sim.py:921, (r + 1) * (1 - spike)).
+
+    A third of the neurons get counts from -7 to 40 -- including counts below
+    -1, which the dynamics never produce, and for which the count after a
+    spike is the reference's -0 -- and half of those a membrane above
+    threshold, so they fire at once: first one step per launch, then in
+    20-step blocks.
+    """
+    name = "batch3_masks"
+    sc, eng = make_engine(name, ring=ring)
+    conn = S.connectome(sc)
+    o = O.Oracle.from_connectome(conn, batch=sc["batch"], params_dict=sc["params"],
+                                 no_refractory=S.driven(sc), seed=sc["seed"])
+    rates = S.rates_matrix(sc)
+    o.rates[:] = rates
+    rt = torch.from_numpy(rates).cuda()
+    n, B = sc["n"], sc["batch"]
+    rng = np.random.default_rng(11)
+    vals = np.array([-7.0, -2.5, -1.5, -1.0, -0.5, -0.0, 0.0, 3.0, 40.0], np.float32)
+
+    def inject():
+        pick = np.sort(rng.choice(n, size=n // 3, replace=False))
+        r = o.refrac.copy()
+        r[:, pick] = rng.choice(vals, size=(B, pick.size))
+        v = o.v.copy()
+        v[:, pick[::2]] = np.float32(eng.v_th + 5.0)
+        o.refrac[:] = r
+        o.v[:] = v
+        eng.refrac.copy_(torch.from_numpy(r))
+        eng.v.copy_(torch.from_numpy(v))
+
+    inject()
+    neg_zero = 0
+    for step in range(6):
+        eng.step(rt)
+        o.run(1)
+        assert np.array_equal(_bits(eng.refrac.cpu().numpy()), _bits(o.refrac)), step
+        assert np.array_equal(_bits(eng.v.cpu().numpy()), _bits(o.v)), step
+        assert np.array_equal(_bits(eng.conductance.cpu().numpy()), _bits(o.conductance)), step
+        neg_zero += int((_bits(o.refrac) == 0x80000000).sum())
+    assert neg_zero > 0  # the case the plain form exists for did occur
+
+    for block in range(3):
+        inject()
+        got = eng.run_block(rt, 40).cpu().numpy()
+        raster = o.run(40, raster=True)
+        bits = np.unpackbits(raster, axis=2, bitorder="little")[:, :, :n]
+        assert np.array_equal(got, bits.sum(0).astype(np.float32)), block
+        assert np.array_equal(_bits(eng.refrac.cpu().numpy()), _bits(o.refrac)), block
+        assert np.array_equal(_bits(eng.v.cpu().numpy()), _bits(o.v)), block
+        assert np.array_equal(_bits(eng.conductance.cpu().numpy()), _bits(o.conductance)), block
+
+
 def test_run_block_equals_stepping():
     """The closed loop's 200-step brain block equals 200 single steps."""
     name = "batch3_masks"
