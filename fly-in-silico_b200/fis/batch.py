@@ -287,15 +287,17 @@ class Batch:
                                for j in range(k)])
         out.copy_(dev, non_blocking=True)
         self.last_d2h_bytes = out.numel() * out.element_size()
+        errs = c.errors_async()
         done = torch.cuda.Event()
         done.record(torch.cuda.current_stream(c.device))
-        return out, done
+        return out, done, errs
 
     def _finish(self, handle):
-        out, done = handle
+        out, done, errs = handle
         done.synchronize()
-        self.core.check_errors()
-        return out.numpy().copy()
+        self.core.raise_errors(errs)
+        # the pinned buffer itself, kept alive by the array: no second copy
+        return out.numpy()
 
     def run(self, specs, timer=None):
         """Run ``specs`` (at most ``capacity``) to completion; host counts per trial.
@@ -311,17 +313,39 @@ class Batch:
     def run_many(self, spec_lists):
         """``run`` over several batches, one after another on the device.
 
-        The host packs the next batch's rows while the device runs the
-        current one, so the device does not wait for the host between
-        batches.  Yields each batch's counts (as ``run`` returns them) as it
-        completes.
+        The device goes from one batch to the next without waiting for the
+        host.  Enqueueing a batch blocks the host until the device's launch
+        queue has room, i.e. until the batch is nearly done, so each batch is
+        enqueued by a worker thread (bound to the caller's device and stream)
+        while this thread packs the next batch's rows; this thread issues no
+        device work until the worker has returned.  A batch's counts (and its
+        error bits) are reduced and copied out in stream order before the next
+        batch's load resets the slots.  Yields each batch's counts (as ``run``
+        returns them) as it completes; ``slots_of_run`` then already
+        describes the batch after it.
         """
+        from concurrent.futures import ThreadPoolExecutor
+
+        dev = self.core.device
+        stream = torch.cuda.current_stream(dev)
+
+        def launch(plan):
+            with torch.cuda.device(dev), torch.cuda.stream(stream):
+                return self._launch(plan)
+
+        it = iter(spec_lists)
+        specs = next(it, None)
+        plan = self._plan(specs) if specs is not None else None
         pending = None
-        for specs in spec_lists:
-            plan = self._plan(specs)          # overlaps the previous batch's run
-            if pending is not None:
-                yield self._finish(pending)
-            pending = self._launch(plan)
+        with ThreadPoolExecutor(max_workers=1) as pool:
+            while plan is not None:
+                job = pool.submit(launch, plan)
+                specs = next(it, None)
+                plan = self._plan(specs) if specs is not None else None  # host only
+                launched = job.result()
+                if pending is not None:
+                    yield self._finish(pending)
+                pending = launched
         if pending is not None:
             yield self._finish(pending)
 

@@ -202,7 +202,19 @@ class Core:
         A CTA whose staged input did not arrive within its bounded wait skipped
         its update and set FIS_ERR_STAGE: the state is then not the model's.
         """
-        err = int(self.done[1].item())
+        self.raise_errors(int(self.done[1].item()))
+
+    def errors_async(self):
+        """The error bits as of this point of the stream, copied into a pinned
+        host word without waiting; pass it to ``raise_errors`` once the stream
+        has passed this point (an event recorded after this call)."""
+        host = torch.empty(1, dtype=torch.int32, pin_memory=True)
+        host.copy_(self.done[1:2], non_blocking=True)
+        return host
+
+    def raise_errors(self, err):
+        """Raise for error bits ``err`` (an int, or a word from ``errors_async``)."""
+        err = int(err[0]) if torch.is_tensor(err) else int(err)
         if err:
             self.done[1].zero_()
             raise RuntimeError("the device reported error bits 0x%x (FIS_ERR_STAGE = 1: "

@@ -178,3 +178,23 @@ def test_run_many_equals_run():
     assert len(got) == len(want)
     for a, b in zip(got, want):
         assert np.array_equal(a, b)
+
+
+def test_run_many_on_a_side_stream():
+    """run_many enqueues on the caller's stream from its worker thread."""
+    import torch
+
+    from fis.batch import Batch
+
+    c = conn()
+    batches = [specs(94, 3, (40, 120)), specs(95, 4, 60), specs(96, 4, (20, 90)),
+               specs(97, 1, 80)]
+    want = [Batch(c, 4, group=2).run(sp) for sp in batches]
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        b = Batch(c, 4, group=2)
+        got = list(b.run_many(iter(batches)))
+    torch.cuda.synchronize()
+    assert len(got) == len(want)
+    for a, w in zip(got, want):
+        assert np.array_equal(a, w)
