@@ -12,6 +12,9 @@ Two sources feed it:
 * :func:`from_weights` -- the reference's own weight object, a torch sparse COO
   ``W[post, pre]`` of signed synapse counts (``data.py:221-226``), so callers of
   ``sim.build_engine(weights=...)`` keep working.
+* :func:`from_parquet` / :func:`from_upstream` -- the upstream connectivity
+  table itself (``data.py:240-259``), read without torch and cached as packed
+  CSR arrays, for when the FlyWire files are at hand.
 
 The kernel format packs one edge into one 32-bit word: the postsynaptic index
 in the high 18 bits and the signed synapse count in the low 14 bits (two's
@@ -183,12 +186,17 @@ def from_weights(weights, n=None) -> Connectome:
         raise ConnectomeError("n = %d but the weight matrix is %s" % (n, tuple(w.shape)))
     idx = w.indices().cpu().numpy()
     val = w.values().detach().cpu().numpy().astype(np.float64)
+    return _from_coo(n, idx[0].astype(np.int64), idx[1].astype(np.int64), val)
+
+
+def _from_coo(n, post, pre, val) -> Connectome:
+    """CSR by pre from coalesced ``(post, pre, value)`` triples (no repeated
+    pair), refusing values that are not integral synapse counts."""
     if val.size and not np.all(val == np.rint(val)):
         frac = float(np.max(np.abs(val - np.rint(val))))
         raise ConnectomeError(
             "weights are not integral synapse counts (largest fractional part "
             "%g); the int32 ring accumulates exact counts only" % frac)
-    post, pre = idx[0].astype(np.int64), idx[1].astype(np.int64)
     cnt = np.rint(val).astype(np.int64)
     nz = cnt != 0
     post, pre, cnt = post[nz], pre[nz], cnt[nz]
@@ -202,6 +210,93 @@ def from_weights(weights, n=None) -> Connectome:
     c = Connectome(n, rp, post.astype(np.int32), cnt.astype(np.int32))
     c.check_bounds()
     return c
+
+
+# Column names and file names of the upstream FlyWire v783 release, as the
+# reference reads them (data.py:43-44, 240-243).
+UPSTREAM_PRE = "Presynaptic_Index"
+UPSTREAM_POST = "Postsynaptic_Index"
+UPSTREAM_VALUE = "Excitatory x Connectivity"
+UPSTREAM_CONN_FILE = "2025_Connectivity_783.parquet"
+UPSTREAM_COMP_FILE = "2025_Completeness_783.csv"
+
+
+def _cache_root() -> Path:
+    return Path(os.environ.get("FIS_CACHE") or (Path(tempfile.gettempdir()) / "fis_cache"))
+
+
+def _csv_rows(path) -> int:
+    """Data rows of a CSV with a header line (the reference's ``len(read_csv)``)."""
+    import csv
+
+    with open(path, newline="") as f:
+        return max(0, sum(1 for _ in csv.reader(f)) - 1)
+
+
+def from_parquet(path, n=None, comp=None, cache=True) -> Connectome:
+    """The upstream connectivity table as a :class:`Connectome` (data.py:221-259).
+
+    ``path``: a parquet file with the columns ``Presynaptic_Index``,
+    ``Postsynaptic_Index`` and ``Excitatory x Connectivity`` (the signed synapse
+    count of the connection).  ``n``: the neuron count, or ``comp``: the
+    completeness CSV, whose row count the reference takes as ``n``.  Repeated
+    (post, pre) pairs are summed, as the reference's ``coalesce()`` does, and
+    pairs summing to zero dropped (they add nothing); values must be integral
+    and indices inside [0, n), else :class:`ConnectomeError`.  The packed CSR
+    arrays are cached on disk (``FIS_CACHE``) keyed by the file's path, size and
+    modification time and by ``n``.
+    """
+    path = Path(path)
+    if n is None:
+        if comp is None:
+            raise ConnectomeError("give n= or comp= (the completeness CSV) for %s" % path)
+        n = _csv_rows(comp)
+    n = int(n)
+    st = path.stat()
+    key = "%s|%d|%d|%d|v1" % (path.resolve(), st.st_size, st.st_mtime_ns, n)
+    cpath = None
+    if cache:
+        cpath = _cache_root() / ("upstream_%s.npz" % hashlib.sha1(key.encode()).hexdigest()[:16])
+        if cpath.exists():
+            try:
+                z = np.load(cpath)
+                c = Connectome(n, z["row_ptr"], z["col"], z["cnt"])
+                c.check_bounds()
+                return c
+            except Exception:
+                pass
+    try:
+        import pyarrow.parquet as pq
+    except ImportError as e:  # pragma: no cover - pyarrow ships with this image
+        raise ImportError("reading the upstream parquet needs pyarrow") from e
+    t = pq.read_table(str(path), columns=[UPSTREAM_PRE, UPSTREAM_POST, UPSTREAM_VALUE])
+    pre = t.column(UPSTREAM_PRE).to_numpy().astype(np.int64)
+    post = t.column(UPSTREAM_POST).to_numpy().astype(np.int64)
+    val = t.column(UPSTREAM_VALUE).to_numpy().astype(np.float32).astype(np.float64)
+    if pre.size and (min(pre.min(), post.min()) < 0 or max(pre.max(), post.max()) >= n):
+        raise ConnectomeError("neuron index outside [0, %d) in %s" % (n, path))
+    # coalesce: one entry per (pre, post), values summed; the key order is
+    # the CSR order (pre major, post ascending)
+    ukey, inv = np.unique(pre * n + post, return_inverse=True)
+    sums = np.bincount(inv.ravel(), weights=val, minlength=ukey.size)
+    c = _from_coo(n, ukey % n, ukey // n, sums)
+    if cpath is not None:
+        try:
+            cpath.parent.mkdir(parents=True, exist_ok=True)
+            tmp = cpath.with_suffix(".tmp.npz")
+            np.savez(tmp, row_ptr=c.row_ptr, col=c.col, cnt=c.cnt)
+            os.replace(tmp, cpath)
+        except OSError:
+            pass
+    return c
+
+
+def from_upstream(data_dir, cache=True) -> Connectome:
+    """``from_parquet`` on an upstream data directory (the reference's
+    ``upstream/data``): its connectivity parquet, ``n`` from its completeness
+    CSV (data.py:43-44, 236-237)."""
+    d = Path(data_dir)
+    return from_parquet(d / UPSTREAM_CONN_FILE, comp=d / UPSTREAM_COMP_FILE, cache=cache)
 
 
 def _out_degrees(rng, n, e, alpha):

@@ -27,6 +27,7 @@ What is different, and why:
 from __future__ import annotations
 
 import json
+import os
 import time
 from dataclasses import asdict, dataclass, field
 from pathlib import Path
@@ -653,13 +654,19 @@ def build_engine(weights=None, neurons=None, silenced=None, params=None, device=
 
     ``weights`` is the reference's sparse ``W[post, pre]`` or a
     :class:`fis.connectome.Connectome`.  The reference loads FlyWire from its
-    data directory when ``weights`` is None; that data is not shipped, so here
-    it is required.
+    data directory when ``weights`` is None (data.py:229-259); here that
+    directory is named by the environment variable ``FIS_FLYWIRE_DATA`` (the
+    upstream ``data`` folder with its connectivity parquet and completeness
+    CSV), and without it ``weights`` is required.
     """
     if weights is None:
-        raise FileNotFoundError(
-            "no connectome given: pass weights= (torch sparse W[post, pre] of synapse "
-            "counts, or fis.connectome.Connectome)")
+        data = os.environ.get("FIS_FLYWIRE_DATA")
+        if not data:
+            raise FileNotFoundError(
+                "no connectome given: pass weights= (torch sparse W[post, pre] of synapse "
+                "counts, or fis.connectome.Connectome), or set FIS_FLYWIRE_DATA to the "
+                "upstream data folder")
+        weights = C.from_upstream(data)
     conn = weights if isinstance(weights, C.Connectome) else C.from_weights(weights)
     n = len(neurons) if neurons is not None else conn.n
     sil = np.asarray(silenced if silenced is not None else [], dtype=np.int64)

@@ -302,3 +302,32 @@ def test_full_size_one_second_rates_match_reference(golden):
     m = compare_rates(counts / 1.0, z["counts"][0] / 1.0)
     assert m["corr"] >= 0.99
     assert np.array_equal(counts, z["counts"][0])  # bit-exact, so in fact identical
+
+
+def test_build_engine_from_the_upstream_folder(tmp_path, monkeypatch):
+    """build_engine(weights=None) reads FIS_FLYWIRE_DATA's upstream tables and
+    steps exactly as the same matrix passed as weights=."""
+    import pyarrow as pa
+    import pyarrow.parquet as pq
+
+    from fis import connectome as C
+    from fis import sim
+
+    sc = S.SCENARIOS["small_b1"]
+    conn = S.connectome(sc)
+    pre = np.repeat(np.arange(conn.n), np.diff(conn.row_ptr))
+    pq.write_table(pa.table({C.UPSTREAM_PRE: pa.array(pre, pa.int64()),
+                             C.UPSTREAM_POST: pa.array(conn.col.astype(np.int64)),
+                             C.UPSTREAM_VALUE: pa.array(conn.cnt.astype(np.float32))}),
+                   str(tmp_path / C.UPSTREAM_CONN_FILE))
+    with open(tmp_path / C.UPSTREAM_COMP_FILE, "w") as fh:
+        fh.write(",root_id\n" + "".join("%d,%d\n" % (i, i) for i in range(conn.n)))
+    monkeypatch.setenv("FIS_CACHE", str(tmp_path / "cache"))
+    monkeypatch.setenv("FIS_FLYWIRE_DATA", str(tmp_path))
+    kw = dict(batch=sc["batch"], seed=sc["seed"], no_refractory=S.driven(sc), graphs=False)
+    a = sim.build_engine(**kw)
+    b = sim.build_engine(weights=conn, **kw)
+    rates = torch.from_numpy(S.rates_matrix(sc)).cuda()
+    for _ in range(60):
+        assert torch.equal(a.step(rates), b.step(rates))
+    assert torch.equal(a.v, b.v) and torch.equal(a.conductance, b.conductance)
