@@ -14,7 +14,12 @@
  * every edge by postsynaptic row (torch.sparse.mm, sim.py:911-913, the
  * reference's default path) and "event" pushes the rows of spiking
  * presynaptic neurons (ev_spmv.cu:60-79).  Both sum integers in float32,
- * which is exact in any order below 2**24 (evspmv.py:957-994).
+ * which is exact in any order below 2**24 (evspmv.py:957-994).  The csrmv
+ * pull accumulates as torch's CPU kernel for a CSR matrix times a dense one
+ * does, one fused multiply-add per entry in ascending column order, so it
+ * also matches the reference bit for bit when a caller has written
+ * fractional spikes (visdyn.py:660-676), where the order and the fusing
+ * decide the last bits.
  *
  * The Bernoulli draw is not torch's generator: the reference's randomness is
  * replaced by a counter-based Philox4x32-10 stream (Salmon et al., SC'11),
@@ -24,8 +29,9 @@
  * Parity of this file is pinned by tests/golden, generated by running the
  * reference's own sim.Engine on the same tapes.
  *
- * Build: gcc -O2 -ffp-contract=off -fno-fast-math -fopenmp -shared -fPIC
+ * Build: gcc -O2 -ffp-contract=off -fno-fast-math -fopenmp -shared -fPIC ... -lm
  */
+#include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -185,7 +191,7 @@ static void core_one_trial(const oracle_ctx* c, const oracle_params* p, int mode
       float acc = 0.0f;
       for (int64_t k = c->t_ptr[post]; k < c->t_ptr[post + 1]; ++k) {
         const int pre = c->t_pre[k];
-        acc += c->t_val[k] * (spikes[o + pre] * m_out[o + pre]);
+        acc = fmaf(c->t_val[k], spikes[o + pre] * m_out[o + pre], acc);
       }
       rec[o + post] = acc;
     }
@@ -290,7 +296,7 @@ int oracle_run(void* h, const oracle_params* p, int batch, int steps, int mode, 
         float acc = 0.0f;
         for (int64_t k = c->t_ptr[post]; k < c->t_ptr[post + 1]; ++k) {
           const int pre = c->t_pre[k];
-          acc += c->t_val[k] * (spikes[o + pre] * m_out[o + pre]);
+          acc = fmaf(c->t_val[k], spikes[o + pre] * m_out[o + pre], acc);
         }
         rec[x] = p->w_scale * acc;
       }

@@ -4,13 +4,14 @@ Runs only where the reference tree is present (it is read, never copied):
 
     python tests/golden/make_golden.py [scenario ...]
 
-For every scenario of ``tests/scenarios.py`` it builds the reference's own
+For every scenario of ``tests/scenarios.py`` (or those named) it builds the reference's own
 ``sim.Engine`` (``lab/flybrain/sim.py:348``) on CPU with the synthetic
 connectome as its weight matrix, silences through the reference's own
 ``sim._silence`` (``sim.py:324-336``), applies the mask plan through
 ``Engine.set_masks`` (``sim.py:510``), and steps it with ``Engine._core``
 (``sim.py:863``) fed by the shared Philox input tape, the way the
-reference's parity probes drive it.  It records the spike raster of every step
+reference's parity probes drive it; a graded scenario first writes its
+fractional values into ``Engine.spikes``, as ``visdyn.py:660-676`` does.  It records the spike raster of every step
 and fingerprints of the full state at milestones, plus the final state arrays
 for the small scenarios.  The fixtures pin the C oracle (CPU tests) and the
 CUDA engine (GPU tests).
@@ -71,6 +72,9 @@ def run_reference(name):
         what = plan.get(step)
         if what is not None:
             eng.set_masks(**S.mask_call(what, idx))
+        gs = S.graded_spikes(sc, step)
+        if gs is not None:
+            eng.spikes[:, torch.from_numpy(gs[0])] = torch.from_numpy(gs[1])
         tape = O.drive_tape(rates, seeds, streams, np.full(B, step, np.int64),
                             sc["params"])
         sp = eng._core(torch.from_numpy(tape)).numpy()

@@ -38,6 +38,13 @@ SCENARIOS = {
                        seed=21, drive_k=320, drive_seed=10, rates=[180.0, 90.0],
                        plan=[(40, "hold_clamp"), (90, "clear"), (150, "all"),
                              (200, "clear")], params=ALT_PARAMS),
+    # Graded spikes (visdyn.py:660-676): before every step, fractional values
+    # in [0, 0.9] are written into the spike state of a seeded set of neurons,
+    # which the reference's csrmv product and refractory update then use.
+    "graded_b2": dict(n=2400, e=2400 * 104, conn_seed=11, batch=2, steps=240, seed=17,
+                      drive_k=300, drive_seed=12, rates=[150.0, 90.0],
+                      plan=[(60, "all"), (150, "clear")], params=None,
+                      graded_k=300, graded_seed=13),
     # The plain single-trial configuration at full size (1,000 steps).
     "full_cfg0": dict(n=138_639, e=15_091_983, conn_seed=0, batch=1, steps=1000,
                       seed=0, drive_k=2249, drive_seed=1, rates=[150.0], plan=[],
@@ -96,3 +103,17 @@ def mask_call(what, idx):
     if what == "hold_clamp":
         return dict(hold=idx[:200], v_clamp=-61.5)
     return {what: idx}
+
+
+def graded_spikes(sc, step):
+    """(neurons, values [batch][k] float32) written into the spike state before
+    ``step`` in a graded scenario, or None."""
+    k = sc.get("graded_k")
+    if not k:
+        return None
+    rng = np.random.default_rng(sc["graded_seed"])
+    idx = np.sort(rng.choice(sc["n"], size=k, replace=False)).astype(np.int64)
+    j = np.arange(k)[None, :]
+    b = np.arange(sc["batch"])[:, None]
+    vals = ((j * 7 + step * 3 + b * 5) % 17) / 17.0 * 0.9
+    return idx, vals.astype(np.float32)

@@ -42,6 +42,9 @@ def run_oracle(name, mode, tape=False):
     for step in range(sc["steps"]):
         if step in plan:
             o.set_masks(**S.mask_call(plan[step], idx))
+        gs = S.graded_spikes(sc, step)
+        if gs is not None:
+            o.spikes[:, gs[0]] = gs[1]
         if tape:
             vs = O.drive_tape(o.rates, o.seeds, o.streams, np.full(sc["batch"], step),
                               sc["params"])
@@ -67,6 +70,26 @@ def test_oracle_matches_reference(name, mode, golden):
     assert int(o.ptr[0]) == int(z["ptr"])
     for k, fps in zip(z["marks_steps"], z["marks"]):
         assert marks[int(k)] == list(fps), int(k)
+
+
+def test_oracle_graded_spikes_match_reference(golden):
+    """Fractional values written into the spike state before every step
+    (visdyn.py:660-676) reach the reference's csrmv product and refractory
+    update; the oracle's fused, ascending-column accumulation gives the
+    reference's bits, signed zeros included."""
+    z = golden("graded_b2")
+    o, raster, marks = run_oracle("graded_b2", O.Oracle.CSRMV)
+    assert np.array_equal(raster, z["raster_bits"])
+    for key, got in (("v", o.v), ("g", o.conductance), ("refrac", o.refrac),
+                     ("spikes", o.spikes), ("ring", o.delay_buffer)):
+        assert np.array_equal(np.ascontiguousarray(got).view(np.uint32),
+                              np.ascontiguousarray(z[key]).view(np.uint32)), key
+    assert int(o.ptr[0]) == int(z["ptr"])
+    for k, fps in zip(z["marks_steps"], z["marks"]):
+        assert marks[int(k)] == list(fps), int(k)
+    # the graded values reached the state: (r + 1) * (1 - s) with a
+    # fractional s leaves fractional refractory counts
+    assert np.any(z["refrac"] != np.round(z["refrac"]))
 
 
 def test_oracle_tape_path_matches(golden):
