@@ -17,7 +17,7 @@ PKG = Path(__file__).resolve().parent
 LIB_NAME = "libfis_b200.so"
 LIB_PATH = PKG / LIB_NAME
 
-FIS_ABI_VERSION = 5
+FIS_ABI_VERSION = 6
 FIS_MAX_BLOCK = 20
 FIS_NOALLOC_RING_INTS = 3 << 20
 REF_EV_ABI = 3
@@ -38,6 +38,7 @@ EXPORTS = ("ev_spmv_i32", "ev_spmv_i64", "ev_spmv_abi", "fis_abi",
            "fis_sizeof_engine", "fis_sizeof_trial", "fis_check", "fis_block",
            "fis_scatter", "fis_update", "fis_advance", "fis_advance_overlap",
            "fis_delay_buffer", "fis_spikes_f32", "fis_load_spikes", "fis_add_rows",
+           "fis_graded_step",
            "fis_ring_row", "fis_block_noalloc")
 
 
@@ -113,6 +114,8 @@ def load(path=None):
     L.fis_spikes_f32.argtypes = [P, I32, I32, I64, P, P]
     L.fis_load_spikes.argtypes = [P, I32, I32, P, P]
     L.fis_add_rows.argtypes = [P, I32, I32, P, I64, I64, P, I64, I64, P]
+    L.fis_graded_step.argtypes = [P, I64, P, P, P, P, P, I32, P, P, P]
+    L.fis_graded_step.restype = ctypes.c_int
     L.fis_block_noalloc.argtypes = [P, I32, I32, I32, P, I32, P]
     L.fis_block_noalloc.restype = ctypes.c_int
     L.fis_ring_row.argtypes = [I32]

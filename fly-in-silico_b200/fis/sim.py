@@ -26,6 +26,7 @@ What is different, and why:
 
 from __future__ import annotations
 
+import ctypes
 import json
 import os
 import time
@@ -236,14 +237,21 @@ def _index(idx, device):
 class Engine:
     """One brain (B trials), held in a state you can step forward.
 
-    Reference: ``sim.Engine`` (sim.py:338-953).
+    Reference: ``sim.Engine`` (sim.py:338-953).  By default the step is the
+    exact integer engine, which carries whole spikes and refuses a caller's
+    write into ``spikes``.  ``graded=True`` opts into the reference's float
+    path for callers that write fractional spikes between steps
+    (visdyn.py:660-676): the csrmv product of the spikes as written, in the
+    reference's summation order, and a float delay ring; one step per call,
+    no CUDA graphs.
     """
 
     STATE_TENSORS = ("v", "conductance", "spikes", "refrac", "delay_buffer")
     MASK_TENSORS = ("m_fire", "m_out", "m_in", "m_hold", "v_hold")
 
     def __init__(self, weights, n, params=None, device="cuda", batch=1, seed=0,
-                 no_refractory=None, spmv=None, allow_inexact=False, group=None, ring=None):
+                 no_refractory=None, spmv=None, allow_inexact=False, group=None, ring=None,
+                 graded=False):
         p = dict(params or MODEL_PARAMS)
         self.p = p
         self.n = int(n)
@@ -302,6 +310,24 @@ class Engine:
         self._ev = None
         self.spmv = name
         self.calls = 0
+        # Graded-spike mode (an explicit opt-in): the reference's float path,
+        # for callers that write fractional values into `spikes` between
+        # steps (visdyn.py:660-676).  The weights as CSR by postsynaptic
+        # neuron (presynaptic indices ascending in a row), the reference's
+        # float delay ring [B][buf_len][N], and the product's scratch.
+        self.graded = bool(graded)
+        if self.graded:
+            dev = c.device
+            pre = np.repeat(np.arange(conn.n, dtype=np.int32), np.diff(conn.row_ptr))
+            order = np.argsort(conn.col, kind="stable")
+            t_ptr = np.zeros(conn.n + 1, dtype=np.int64)
+            np.cumsum(np.bincount(conn.col, minlength=conn.n), out=t_ptr[1:])
+            self._t_csr = (torch.from_numpy(t_ptr).to(dev),
+                           torch.from_numpy(np.ascontiguousarray(pre[order])).to(dev),
+                           torch.from_numpy(conn.cnt[order].astype(np.float32)).to(dev))
+            self._fring = torch.zeros((self.batch, self.buf_len, self.n), dtype=torch.float32,
+                                      device=dev)
+            self._rec = torch.empty((self.batch, self.n), dtype=torch.float32, device=dev)
 
     # --- views of the engine's own state ---------------------------------
 
@@ -315,6 +341,8 @@ class Engine:
 
     @property
     def delay_buffer(self):
+        if self.graded:
+            return self._fring
         return self.core.delay_buffer()
 
     def _mask(self, bit):
@@ -428,7 +456,31 @@ class Engine:
         if self.spikes._version != self._spikes_version:
             raise RuntimeError(
                 "Engine.spikes was written by the caller; graded or edited spikes are not "
-                "supported by the exact integer engine (restore() sets a 0/1 spike state)")
+                "supported by the exact integer engine (restore() sets a 0/1 spike state; "
+                "build the engine with graded=True for the reference's float path)")
+
+    def _graded_step(self, rates=None, vstim=None):
+        """One step of the graded-spike mode (fis_graded_step): the product of
+        the spikes as they are now, fractional values included."""
+        c = self.core
+        c._sync_trials()
+        t_ptr, t_pre, t_val = self._t_csr
+        saved = c.desc.rates
+        if rates is not None:
+            c.desc.rates = rates.data_ptr()
+        try:
+            rc = c.lib.fis_graded_step(
+                ctypes.byref(c.desc), c.step, ctypes.c_void_p(t_ptr.data_ptr()),
+                ctypes.c_void_p(t_pre.data_ptr()), ctypes.c_void_p(t_val.data_ptr()),
+                ctypes.c_void_p(self.spikes.data_ptr()), ctypes.c_void_p(self._fring.data_ptr()),
+                self.ptr, ctypes.c_void_p(self._rec.data_ptr()),
+                ctypes.c_void_p(vstim.data_ptr()) if vstim is not None else None,
+                ctypes.c_void_p(torch.cuda.current_stream(c.device).cuda_stream))
+        finally:
+            c.desc.rates = saved
+        _lib.check(rc, "fis_graded_step")
+        c.step += 1
+        self.calls += 1
 
     def _rates_arg(self, rates):
         c = self.core
@@ -441,6 +493,9 @@ class Engine:
 
     def step(self, rates):
         """Advance one 0.1 ms tick; ``rates`` [batch, n] in Hz (sim.py:745-771)."""
+        if self.graded:
+            self._graded_step(rates=self._rates_arg(rates))
+            return self.spikes
         self._check_spikes_untouched()
         self.calls += 1
         c = self.core
@@ -465,6 +520,9 @@ class Engine:
         The reference's deterministic half of the step (sim.py:863-953): the
         caller supplies ``voltage_stim`` [batch, n] (``w * (bern * gain)``).
         """
+        if self.graded:
+            self._graded_step(vstim=self._rates_arg(voltage_stim))
+            return self.spikes
         self._check_spikes_untouched()
         c = self.core
         vs = self._rates_arg(voltage_stim)
@@ -483,8 +541,16 @@ class Engine:
         engine.step(rates)[0]`` 200 times per 20 ms control step) as one call:
         the steps run in 20-step fused blocks and the spikes are summed on the
         device by the update kernel, with no host work between steps.  Equal to
-        stepping one by one; ``spikes`` holds the last step afterwards.
+        stepping one by one; ``spikes`` holds the last step afterwards.  In
+        graded-spike mode the steps run one by one.
         """
+        if self.graded:
+            r = self._rates_arg(rates)
+            acc = torch.zeros((self.batch, self.n), dtype=torch.float32, device=self.core.device)
+            for _ in range(int(steps)):
+                self._graded_step(rates=r)
+                acc += self.spikes
+            return acc
         self._check_spikes_untouched()
         c = self.core
         r = self._rates_arg(rates)
@@ -511,7 +577,10 @@ class Engine:
         return acc.to(torch.float32)
 
     def use_graphs(self, enable=True):
-        """Capture the step into a CUDA graph (sim.py:634-743)."""
+        """Capture the step into a CUDA graph (sim.py:634-743).  Returns
+        whether graphs are in use; the graded-spike mode steps without them."""
+        if self.graded:
+            return False
         if not enable:
             self._graphs = self._vstim = self._pool = None
             return False
@@ -606,14 +675,18 @@ class Engine:
 
         v, g, refrac = arr("v"), arr("conductance"), arr("refrac")
         spikes = arr("spikes")
-        if not bool(((spikes == 0) | (spikes == 1)).all()):
-            raise ValueError("spikes must be 0/1: the integer ring carries whole spikes only")
         ring = arr("delay_buffer")
-        w = np.float32(self.w_scale)
-        counts = torch.round(ring / float(w)).to(torch.int32)
-        back = (counts.to(torch.float32) * float(w))
-        if not bool((back == ring).all()):
-            raise ValueError("delay_buffer holds values that are not w_scale * integer counts")
+        counts = None
+        if not self.graded:
+            if not bool(((spikes == 0) | (spikes == 1)).all()):
+                raise ValueError("spikes must be 0/1: the integer ring carries whole spikes "
+                                 "only (the graded-spike mode takes any values)")
+            w = np.float32(self.w_scale)
+            counts = torch.round(ring / float(w)).to(torch.int32)
+            back = (counts.to(torch.float32) * float(w))
+            if not bool((back == ring).all()):
+                raise ValueError("delay_buffer holds values that are not w_scale * integer "
+                                 "counts (the graded-spike mode takes any values)")
         ptr = int(state["ptr"]) % self.buf_len if want("ptr") else self.ptr
         if want("gen"):
             rec = PhiloxState.parse(state["gen"])
@@ -634,7 +707,14 @@ class Engine:
             c.trials[b].start = t - int(own[b])
         c.mark_trials()
         c._sync_trials()
-        c.load_state(t, v=v, g=g, refrac=refrac, spikes=spikes, ring_counts=counts)
+        if self.graded:
+            c.set_clock(t)
+            c.v.copy_(v)
+            c.g.copy_(g)
+            c.refrac.copy_(refrac)
+            self._fring.copy_(ring)
+        else:
+            c.load_state(t, v=v, g=g, refrac=refrac, spikes=spikes, ring_counts=counts)
         self.spikes.copy_(spikes)
         self._spikes_version = self.spikes._version
         for name in self.STATE_TENSORS:
@@ -649,7 +729,7 @@ class Engine:
 
 def build_engine(weights=None, neurons=None, silenced=None, params=None, device=None,
                  batch=1, seed=0, no_refractory=None, graphs=True, spmv=None,
-                 allow_inexact=False, group=None, ring=None):
+                 allow_inexact=False, group=None, ring=None, graded=False):
     """Return a ready :class:`Engine` (sim.py:956-987).
 
     ``weights`` is the reference's sparse ``W[post, pre]`` or a
@@ -657,7 +737,8 @@ def build_engine(weights=None, neurons=None, silenced=None, params=None, device=
     data directory when ``weights`` is None (data.py:229-259); here that
     directory is named by the environment variable ``FIS_FLYWIRE_DATA`` (the
     upstream ``data`` folder with its connectivity parquet and completeness
-    CSV), and without it ``weights`` is required.
+    CSV), and without it ``weights`` is required.  ``graded=True`` builds the
+    graded-spike mode of :class:`Engine`.
     """
     if weights is None:
         data = os.environ.get("FIS_FLYWIRE_DATA")
@@ -673,7 +754,7 @@ def build_engine(weights=None, neurons=None, silenced=None, params=None, device=
     conn = conn.without(sil)
     eng = Engine(conn, n, params=params, device=device or "cuda", batch=batch, seed=seed,
                  no_refractory=no_refractory, spmv=spmv, allow_inexact=allow_inexact,
-                 group=group, ring=ring)
+                 group=group, ring=ring, graded=graded)
     if graphs:
         eng.use_graphs()
     return eng

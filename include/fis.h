@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define FIS_ABI_VERSION 5
+#define FIS_ABI_VERSION 6
 
 /* Largest number of steps one block may advance (registers per thread). */
 #define FIS_MAX_BLOCK 20
@@ -296,6 +296,30 @@ int fis_add_rows(const fis_engine* e, int32_t nb, int32_t rows,
                  const int32_t* src, int64_t src_row_stride,
                  int64_t src_trial_stride, int32_t* dst, int64_t dst_row_stride,
                  int64_t dst_trial_stride, void* stream);
+
+/*
+ * Graded-spike mode: one step of the reference's float path (sim.py:863-953
+ * with the csrmv product of sim.py:910-913) for callers that write fractional
+ * values into the spike state (visdyn.py:660-676), where whole-spike integer
+ * counts no longer describe the input.  All trials [0, batch) of `e` advance
+ * one step:
+ *   recurrent[b][post] = w_scale * sum over in-edges, ascending pre, of
+ *                        val * (spikes[b][pre] * m_out[b][pre]), one fused
+ *                        multiply-add per edge (torch's CPU csrmv order)
+ *   then the step with ring[b][ptr] as the delayed input, which the slot
+ *   then takes over from `recurrent`; spikes[b] becomes the new 0/1 spikes.
+ * e's v, g, refrac, flags (masks, silencing, no-refractory), rates, trials
+ * (seed, lane, start, clamp value) and params are used as by fis_block; the
+ * drive is e's Philox draw for global step `step`, or `vstim` [B][N] when
+ * non-null.  t_ptr int64 [N+1] / t_pre int32 [E] / t_val float [E]: the
+ * weights W[post, pre] as CSR by postsynaptic neuron, presynaptic indices
+ * ascending within a row.  spikes float [B][N] (read, then written), ring
+ * float [B][buf_len][N], rec float [B][N] scratch; 0 <= ptr < buf_len.
+ * Replaces Engine._core's float path (sim.py:863-953) for graded spikes.
+ */
+int fis_graded_step(const fis_engine* e, int64_t step, const int64_t* t_ptr,
+                    const int32_t* t_pre, const float* t_val, float* spikes, float* ring,
+                    int32_t ptr, float* rec, const float* vstim, void* stream);
 
 /* Row length NR of the scratch ring for N neurons (N rounded up to 256). */
 int fis_ring_row(int32_t n);
