@@ -21,7 +21,11 @@ What is different, and why:
   flag byte per neuron); ``restore`` is the way to change them;
 * ``use_graphs`` captures one CUDA graph (the device keeps its own step
   counter, so one graph serves every ring position, where the reference
-  needs 19).
+  needs 19);
+* writing into ``spikes`` between steps (graded values, visdyn.py:660-676)
+  raises unless the engine was built with ``graded=True``, which selects the
+  reference's float path (its csrmv summation order, a float and writable
+  ``delay_buffer``, no CUDA graphs) instead of the exact integer engine.
 """
 
 from __future__ import annotations
