@@ -65,6 +65,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true",
                     help="skip the uneven-duration and serving measurements")
+    ap.add_argument("--block-steps", type=int, default=None,
+                    help="steps per block (1-20; default 20, the delay lag): shorter blocks "
+                         "separate the update's per-block cost from its per-step cost")
     return ap.parse_args()
 
 
@@ -275,7 +278,13 @@ def main():
         best = tune(conn, args.trials)
     else:
         best = {"group": args.group, "chunk": None, "candidates": []}
-    batch = Batch(conn, args.trials, group=best["group"], chunk=best["chunk"])
+    core = None
+    if args.block_steps is not None:
+        from fis.engine import Core
+
+        core = Core(conn, args.trials, group=best["group"], chunk=best["chunk"], raster=False,
+                    max_block=args.block_steps)
+    batch = Batch(conn, args.trials, group=best["group"], chunk=best["chunk"], core=core)
     core = batch.core
     slots = list(range(args.trials))
     batch.load(slots, specs)

@@ -364,6 +364,20 @@ class Core:
         nrows = self.batch if rows is None else max(1, min(int(rows), self.batch))
         if self.pending is not None or timer is not None or self.max_block != min(
                 _lib.FIS_MAX_BLOCK, self.lag):
+            if events and timer is None:
+                # the native loop's event pairs, around every `every`-th update
+                # launch, recorded on the current stream that block() uses
+                n_pairs, every, seen = len(events) // 2, max(1, int(every)), [0]
+                for e in events:  # pairs never reached read as zero, as natively
+                    e.record(torch.cuda.current_stream(self.device))
+
+                def timer(_stream, start):
+                    j, r = divmod(seen[0], every)
+                    if r == 0 and j < n_pairs:
+                        events[2 * j + (0 if start else 1)].record(
+                            torch.cuda.current_stream(self.device))
+                    if not start:
+                        seen[0] += 1
             left = steps
             while left > 0:
                 k = min(left, self.max_block)
