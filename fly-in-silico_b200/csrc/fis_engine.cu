@@ -907,18 +907,22 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
   // Without the full raster only the last step's words are kept (the next
   // block reads them for the refractory reset); the partial and tape loops
   // always store every step.
+  // The last step's words are the warp's ballots of keep == 0, which every
+  // lane holds: lane 0 stores them directly.
   const bool only_last = !E.raster && full && !kTape;
   if (only_last) {
     float k0, k1;
     up2(st.keep, k0, k1);
     const uint32_t w0 = __ballot_sync(0xFFFFFFFFu, k0 == 0.f);
     const uint32_t w1 = __ballot_sync(0xFFFFFFFFu, k1 == 0.f);
-    if (lane == 0) {
-      sb0[K - 1] = w0;
-      sb1[K - 1] = w1;
+    if (lane == 0 && warp_valid) {
+      const int sl = slot0 + K - 1 < L ? slot0 + K - 1 : slot0 + K - 1 - L;
+      if (runs[0]) bitrow[0][sl] = w0;
+      if (runs[1]) bitrow[1][sl] = w1;
     }
+  } else {
+    __syncwarp();
   }
-  __syncwarp();
 
   float ov[2], og[2], orr[2], okeep[2], ospk[2];
   up2(st.v, ov[0], ov[1]);
@@ -931,7 +935,7 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
     if (!runs[t]) continue;
     const int b = b0 + 2 * pp + t;
     // the raster words of the K steps into the ring of the last L steps
-    if ((only_last ? lane == K - 1 : lane < K) && warp_valid) {
+    if (!only_last && lane < K && warp_valid) {
       const int sl = slot0 + lane < L ? slot0 + lane : slot0 + lane - L;
       bitrow[t][sl] = sbal[t][wib][lane];
     }
