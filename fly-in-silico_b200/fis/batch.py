@@ -126,6 +126,7 @@ class Batch:
                                  chunk=chunk, raster=False)
         self.n = self.core.n
         self.capacity = self.core.batch
+        self._copy_stream = None  # the side stream of the counts' copy to the host
         self._recs = {}                          # index -> int32 [n_bins][N]
         self._rec_refs = {}                      # index -> trials recording into it
         self._slot_rec = [None] * self.capacity  # slot -> index
@@ -285,11 +286,21 @@ class Batch:
         else:
             dev = torch.stack([self.recording(self.slots_of_run[j]).sum(0, dtype=torch.int32)
                                for j in range(k)])
-        out.copy_(dev, non_blocking=True)
+        # The copy to the host (and of the error bits) runs on a side stream,
+        # after the run, so that the next run's kernels do not queue behind it.
+        ready = torch.cuda.Event()
+        ready.record(torch.cuda.current_stream(c.device))
+        if self._copy_stream is None:
+            self._copy_stream = torch.cuda.Stream(c.device)
+        cs = self._copy_stream
+        cs.wait_event(ready)
+        with torch.cuda.stream(cs):
+            out.copy_(dev, non_blocking=True)
+            errs = c.errors_async()
+            done = torch.cuda.Event()
+            done.record(cs)
+        dev.record_stream(cs)
         self.last_d2h_bytes = out.numel() * out.element_size()
-        errs = c.errors_async()
-        done = torch.cuda.Event()
-        done.record(torch.cuda.current_stream(c.device))
         return out, done, errs
 
     def _finish(self, handle):
