@@ -29,7 +29,9 @@
  * Parity of this file is pinned by tests/golden, generated by running the
  * reference's own sim.Engine on the same tapes.
  *
- * Build: gcc -O2 -ffp-contract=off -fno-fast-math -fopenmp -shared -fPIC ... -lm
+ * Build: gcc -O2 -mfma -ffp-contract=off -fno-fast-math -fopenmp -shared -fPIC ... -lm
+ * (-mfma makes fmaf the hardware instruction; -ffp-contract=off keeps every
+ * other product and sum rounded on its own)
  */
 #include <math.h>
 #include <stdint.h>
