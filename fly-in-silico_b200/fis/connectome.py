@@ -136,6 +136,17 @@ class Connectome:
             raise ConnectomeError("connectome fails its bounds check:\n  "
                                   + "\n  ".join(bad))
 
+    def by_post(self):
+        """The weights as CSR by postsynaptic neuron: ``(t_ptr`` int64 [n+1],
+        ``t_pre`` int32 [E], ``t_val`` float32 [E]``)``, presynaptic indices
+        ascending within a row -- torch's CSR of ``W[post, pre]``, the layout
+        and order of the reference's csrmv pull (``sim.py:357, 910-913``)."""
+        pre = np.repeat(np.arange(self.n, dtype=np.int32), np.diff(self.row_ptr))
+        order = np.argsort(self.col, kind="stable")
+        t_ptr = np.zeros(self.n + 1, dtype=np.int64)
+        np.cumsum(np.bincount(self.col, minlength=self.n), out=t_ptr[1:])
+        return t_ptr, np.ascontiguousarray(pre[order]), self.cnt[order].astype(np.float32)
+
     def to_torch_weights(self, device="cpu"):
         """The reference's weight object: sparse COO ``W[post, pre]`` float32."""
         import torch

@@ -322,13 +322,7 @@ class Engine:
         self.graded = bool(graded)
         if self.graded:
             dev = c.device
-            pre = np.repeat(np.arange(conn.n, dtype=np.int32), np.diff(conn.row_ptr))
-            order = np.argsort(conn.col, kind="stable")
-            t_ptr = np.zeros(conn.n + 1, dtype=np.int64)
-            np.cumsum(np.bincount(conn.col, minlength=conn.n), out=t_ptr[1:])
-            self._t_csr = (torch.from_numpy(t_ptr).to(dev),
-                           torch.from_numpy(np.ascontiguousarray(pre[order])).to(dev),
-                           torch.from_numpy(conn.cnt[order].astype(np.float32)).to(dev))
+            self._t_csr = tuple(torch.from_numpy(a).to(dev) for a in conn.by_post())
             self._fring = torch.zeros((self.batch, self.buf_len, self.n), dtype=torch.float32,
                                       device=dev)
             self._rec = torch.empty((self.batch, self.n), dtype=torch.float32, device=dev)

@@ -1,9 +1,11 @@
-"""The upstream-table connectome loader (lab/flybrain/data.py:221-259), on CPU.
+"""Connectome loading and layouts against the reference's own objects, on CPU.
 
-Small tables in the upstream column layout, with repeated (pre, post) pairs
-and a pair that sums to zero, loaded by ``from_parquet`` and compared with the
-reference's own object for the same table -- a coalesced torch sparse COO
-``W[post, pre]`` -- through ``from_weights``, and with a dense sum.
+The upstream-table loader (lab/flybrain/data.py:221-259): small tables in the
+upstream column layout, with repeated (pre, post) pairs and a pair that sums
+to zero, loaded by ``from_parquet`` and compared with the reference's object
+for the same table -- a coalesced torch sparse COO ``W[post, pre]`` -- through
+``from_weights``, and with a dense sum.  The CSR by postsynaptic neuron of the
+graded-spike mode, compared with torch's CSR of ``W`` (the reference's csrmv).
 """
 
 import numpy as np
@@ -103,3 +105,15 @@ def test_refusals(tmp_path):
         C.from_parquet(g, n=n, cache=False)
     with pytest.raises(C.ConnectomeError, match="n="):
         C.from_parquet(g, cache=False)
+
+
+def test_by_post_is_torchs_csr_of_w():
+    """The graded mode's pull layout is torch's CSR of W[post, pre], the one the
+    reference's csrmv reads (sim.py:357): same row pointers, column order and
+    values."""
+    c = C.synthetic(n=700, e=700 * 40, seed=4, cache=False)
+    t_ptr, t_pre, t_val = c.by_post()
+    w = c.to_torch_weights().to_sparse_csr()
+    assert np.array_equal(t_ptr, w.crow_indices().numpy())
+    assert np.array_equal(t_pre, w.col_indices().numpy())
+    assert np.array_equal(t_val, w.values().numpy())
