@@ -98,16 +98,22 @@ def sparse_rows(specs, n, slots):
     fb = np.concatenate(f_bits) if f_bits else u8
     ra = np.concatenate(r_at) if r_at else i64
     rv = np.concatenate(r_val) if r_val else f32
-    if fa.size:
+    # One stable sort per array (skipped when the positions already ascend,
+    # as a trial's sorted stimulus set in ascending slots does); runs of a
+    # repeated position then merge: flag bits OR together, and a rate keeps
+    # its last value, as an indexed assignment does.
+    if fa.size and not np.all(fa[1:] > fa[:-1]):
         order = np.argsort(fa, kind="stable")
         fa, fb = fa[order], fb[order]
-        fa, first = np.unique(fa, return_index=True)
+        first = np.flatnonzero(np.concatenate(([True], fa[1:] != fa[:-1])))
+        fa = fa[first]
         fb = np.bitwise_or.reduceat(fb, first)
-    if ra.size:  # keep the last of repeated positions
-        rev_at, rev_first = np.unique(ra[::-1], return_index=True)
-        rv = rv[::-1][rev_first]
-        ra = rev_at
-    return fa, fb, ra, rv
+    if ra.size and not np.all(ra[1:] > ra[:-1]):
+        order = np.argsort(ra, kind="stable")
+        ra, rv = ra[order], rv[order]
+        last = np.flatnonzero(np.concatenate((ra[1:] != ra[:-1], [True])))
+        ra, rv = ra[last], rv[last]
+    return fa, fb, ra, np.ascontiguousarray(rv)
 
 
 class Batch:
