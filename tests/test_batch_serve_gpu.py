@@ -198,3 +198,23 @@ def test_run_many_on_a_side_stream():
     assert len(got) == len(want)
     for a, w in zip(got, want):
         assert np.array_equal(a, w)
+
+
+def test_run_many_raises_a_batch_error_when_its_counts_are_due():
+    """run_many reads each batch's error bits with its counts (copied in stream
+    order, no host wait): a batch whose staging waits ran out raises at its
+    yield, with the next batch already enqueued; the context stays usable."""
+    from fis.batch import Batch
+
+    c = conn()
+    sp = specs(72, 2, 40)
+    b = Batch(c, 2, group=2)
+    b.core.desc.wait_polls = 2000
+    b.core.desc.inject_stall = 1    # no staging copy is issued: every wait runs out
+    it = b.run_many([sp, sp])
+    with pytest.raises(RuntimeError, match="error bits"):
+        next(it)
+    torch.cuda.synchronize()
+    fresh = Batch(c, 2, group=2).run(sp)
+    for j, s in enumerate(sp):
+        assert np.array_equal(fresh[j], oracle_trial(c, s)[1]), j
