@@ -440,9 +440,12 @@ k_scatter(const fis_engine E, const ScatterArgs A) {
 
 // Phase A of a block as one grid: CTAs [0, scat) scatter, the rest draw the
 // Poisson drive.  Both are latency-bound; in one grid their CTAs share the
-// SMs and fill each other's waits, and the block needs one launch less.
+// SMs and fill each other's waits, and the block needs one launch less.  It
+// runs beside the previous group's update, whose CTAs fill the register
+// file: at 32 registers a thread (a few bytes of the Philox draw spill to L1)
+// two phase-A CTAs take the room of one update CTA instead of 1.5.
 static_assert(kScatThreads == kDriveThreads, "one block size for both roles");
-__global__ void __launch_bounds__(kScatThreads)
+__global__ void __launch_bounds__(kScatThreads, 7)
 k_phase_a(const fis_engine E, const ScatterArgs A, const int scat) {
   extern __shared__ int32_t pre_sum[];
   if ((int)blockIdx.x < scat)
