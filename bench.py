@@ -41,12 +41,12 @@ SPEC_SEED = 2024
 CONN_SEED = 0
 # Update-kernel DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum)
 # per trial-neuron and block, from the ncu capture summarised in
-# profiles/k_update_batched64.md (187.7 MB for one launch of 16 trials x
+# profiles/k_update_batched64.md (187.0 MB for one launch of 16 trials x
 # 138,639 neurons x 20 steps at steady activity; ncu flushes caches between
 # replay passes, so this counts the L2-resident scratch ring as cold reads and
 # its clearing as DRAM writes, an upper bound).  Scaled to the bench's launch
 # size by the neurons it processes.
-NCU_TRAFFIC_PER_NEURON_BLOCK = 187.74e6 / (16 * 138_639)
+NCU_TRAFFIC_PER_NEURON_BLOCK = 187.04e6 / (16 * 138_639)
 # Algorithmic HBM bytes of the update per trial-neuron and block: state
 # v, g, refrac read and written (24), flags (1), rates (4), kick steps (4),
 # and the previous and last step's raster bits (2/8).
