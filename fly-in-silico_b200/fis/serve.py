@@ -71,7 +71,8 @@ class Server:
     """Slots on one GPU, filled from a queue as they free up."""
 
     def __init__(self, conn: Connectome, capacity: int = 256, params=None, device="cuda",
-                 group=None, chunk=None, memory_budget: int | None = None):
+                 group=None, chunk=None, memory_budget: int | None = None,
+                 advance_steps: int = 200):
         self.batch = Batch(conn, capacity, params=params, device=device, group=group,
                            chunk=chunk)
         self.core = self.batch.core
@@ -91,6 +92,10 @@ class Server:
         for b in range(capacity):             # idle slots: never active
             self.core.trials[b].start = self.core.trials[b].end = 0
         self.core.mark_trials()
+        # steps enqueued per turn of the serving loop (cut at the next trial
+        # end): new arrivals wait at most this long for admission
+        self.advance_steps = max(1, int(advance_steps))
+        self._in_flight = None                # event after the previous turn's work
         self.clock0 = time.perf_counter()
 
     # --- host side --------------------------------------------------------
@@ -161,17 +166,26 @@ class Server:
         return hi
 
     def step_block(self):
-        """One block of the engine for everything running (up to 20 steps).
+        """Advance everything running by up to ``advance_steps`` steps.
 
-        The block is cut at the next trial end, so every request finishes
-        exactly on a block boundary.
+        The stretch is cut at the next trial end, so every request finishes
+        exactly on a block boundary, and it runs as the engine's native block
+        loop (one library call, trial groups overlapped) rather than block by
+        block from Python, whose per-block host cost exceeds the device time of
+        a block when few trials run.  At most two stretches are in flight: the
+        host waits for the previous one before enqueueing another, so a
+        request admitted now does not queue behind a long backlog.
         """
         if not self.running:
             return 0
         ends = [end for _, _, end, _, _ in self.running.values()]
-        k = min(self.core.max_block, min(ends) - self.core.step)
-        k = max(1, k)
-        self.core.block(k, rows=self._active_rows())
+        k = max(1, min(self.advance_steps, min(ends) - self.core.step))
+        self.core.advance(k, rows=self._active_rows())
+        done = torch.cuda.Event()
+        done.record(torch.cuda.current_stream(self.core.device))
+        if self._in_flight is not None:
+            self._in_flight.synchronize()
+        self._in_flight = done
         return k
 
     # --- driving ------------------------------------------------------------
