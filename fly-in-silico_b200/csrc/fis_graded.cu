@@ -12,13 +12,21 @@
 // [B][buf_len][N] with the reference's read-then-write slot `ptr`.  Two
 // kernels per step:
 //
-//  * k_graded_pull: one thread per (trial, postsynaptic neuron) walks the
-//    neuron's in-edges in ascending presynaptic order and accumulates with one
-//    fused multiply-add per edge -- the order and fusing of torch's CPU kernel
-//    for a CSR matrix times a dense one, which the reference's csrmv path runs,
-//    so the sums carry the reference's bits.  Terms with a zero factor are
-//    skipped: fma(v, +-0, acc) = acc for every acc the loop can hold (it starts
-//    at +0 and a rounded sum is -0 only when both addends are -0).
+//  * k_graded_nz marks, per trial, the neurons whose spikes * m_out is not
+//    zero, one bit each;
+//  * k_graded_pull: one warp per (trial, postsynaptic neuron) accumulates the
+//    neuron's in-edges in ascending presynaptic order with one fused
+//    multiply-add per edge -- the order and fusing of torch's CPU kernel for a
+//    CSR matrix times a dense one, which the reference's csrmv path runs, so
+//    the sums carry the reference's bits.  Terms with a zero factor change
+//    nothing: fma(v, +-0, acc) = acc for every acc the chain can hold (it
+//    starts at +0, and a rounded sum is -0 only when both addends are -0).
+//    So each CTA holds its trial's bit mask in shared memory; a warp streams
+//    32 consecutive presynaptic indices of the row at a time, tests them in
+//    the mask, and gathers value and weight only for the few set ones (spikes
+//    are rare and graded values sit on a few hundred neurons), folding them
+//    lowest lane (lowest presynaptic index) first, every lane carrying the
+//    same sum.
 //  * k_graded_step: one thread per (trial, neuron), the reference's
 //    operations in its order, one float32 rounding at a time; masks, the
 //    refractory steps and the Poisson drive come from the engine's flag bits,
@@ -39,25 +47,63 @@ namespace {
 
 constexpr int kGradedThreads = 256;
 
+// spikes * m_out (sim.py:912): m_out is 0 for a neuron whose output is cut or
+// which is silenced in this trial
+__device__ __forceinline__ float graded_x(const float* spikes, const uint8_t* flags, int64_t at) {
+  const float m = (flags[at] & (FIS_FL_OUT_OFF | FIS_FL_SILENCED)) ? 0.f : 1.f;
+  return __fmul_rn(spikes[at], m);
+}
+
+// nz[b][i / 32] bit i % 32: spikes * m_out of neuron i in trial b is not zero
+__global__ void __launch_bounds__(kGradedThreads)
+k_graded_nz(const float* __restrict__ spikes, const uint8_t* __restrict__ flags, const int n,
+            const int words, uint32_t* __restrict__ nz) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t o = (int64_t)blockIdx.y * n;
+  const bool on = i < n && graded_x(spikes, flags, o + i) != 0.f;
+  const uint32_t word = __ballot_sync(0xFFFFFFFFu, on);
+  if ((threadIdx.x & (kWarp - 1)) == 0 && (i >> 5) < words)
+    nz[(int64_t)blockIdx.y * words + (i >> 5)] = word;
+}
+
 __global__ void __launch_bounds__(kGradedThreads)
 k_graded_pull(const int64_t* __restrict__ t_ptr, const int32_t* __restrict__ t_pre,
               const float* __restrict__ t_val, const float* __restrict__ spikes,
-              const uint8_t* __restrict__ flags, const int n, const float w,
-              float* __restrict__ rec) {
-  const int post = blockIdx.x * blockDim.x + threadIdx.x;
-  if (post >= n) return;
-  const int64_t o = (int64_t)blockIdx.y * n;
-  float acc = 0.f;
-  const int64_t k1 = t_ptr[post + 1];
-  for (int64_t k = t_ptr[post]; k < k1; ++k) {
-    const int pre = t_pre[k];
-    // spikes * m_out (sim.py:912): m_out is 0 for a neuron whose output is
-    // cut or which is silenced in this trial
-    const float m = (flags[o + pre] & (FIS_FL_OUT_OFF | FIS_FL_SILENCED)) ? 0.f : 1.f;
-    const float x = __fmul_rn(spikes[o + pre], m);
-    if (x != 0.f) acc = __fmaf_rn(t_val[k], x, acc);
+              const uint8_t* __restrict__ flags, const uint32_t* __restrict__ nz,
+              const int n, const int words, const float w, float* __restrict__ rec) {
+  extern __shared__ uint32_t smask[];  // this trial's nz words
+  const int b = blockIdx.y;
+  const int64_t o = (int64_t)b * n;
+  for (int j = threadIdx.x; j < words; j += blockDim.x) smask[j] = nz[(int64_t)b * words + j];
+  __syncthreads();
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int warps = kGradedThreads / kWarp;
+  for (int post = blockIdx.x * warps + (int)(threadIdx.x / kWarp); post < n;
+       post += gridDim.x * warps) {  // warp-uniform
+    float acc = 0.f;
+    const int64_t k0 = t_ptr[post], k1 = t_ptr[post + 1];
+    for (int64_t base = k0; base < k1; base += kWarp) {
+      const int64_t k = base + lane;
+      int pre = 0;
+      bool on = false;
+      if (k < k1) {
+        pre = t_pre[k];
+        on = (smask[pre >> 5] >> (pre & 31)) & 1u;
+      }
+      unsigned bits = __ballot_sync(0xFFFFFFFFu, on);
+      float v = 0.f, x = 0.f;
+      if (on) {
+        v = t_val[k];
+        x = graded_x(spikes, flags, o + pre);
+      }
+      while (bits) {
+        const int j = __ffs(bits) - 1;
+        bits &= bits - 1;
+        acc = __fmaf_rn(__shfl_sync(0xFFFFFFFFu, v, j), __shfl_sync(0xFFFFFFFFu, x, j), acc);
+      }
+    }
+    if (lane == 0) rec[o + post] = __fmul_rn(w, acc);
   }
-  rec[o + post] = __fmul_rn(w, acc);
 }
 
 __global__ void __launch_bounds__(kGradedThreads)
@@ -135,8 +181,27 @@ int fis_graded_step(const fis_engine* e, int64_t step, const int64_t* t_ptr,
   if (e->p.buf_len < 1 || ptr < 0 || ptr >= e->p.buf_len) return FIS_E_BOUNDS;
   cudaStream_t st = (cudaStream_t)stream;
   const dim3 grid((e->n + kGradedThreads - 1) / kGradedThreads, e->batch);
-  k_graded_pull<<<grid, kGradedThreads, 0, st>>>(t_ptr, t_pre, t_val, spikes, e->flags, e->n,
-                                                 e->p.w_scale, rec);
+  // the nonzero mask lives after the [B][N] product in the scratch
+  const int words = (e->n + kWarp - 1) / kWarp;
+  uint32_t* nz = reinterpret_cast<uint32_t*>(rec + (int64_t)e->batch * e->n);
+  k_graded_nz<<<grid, kGradedThreads, 0, st>>>(spikes, e->flags, e->n, words, nz);
+  // a few CTAs per SM share the rows of a trial, each loading the mask once
+  int sms = 0, dev = 0;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
+    sms = 148;
+  const int per_trial = (sms * 8 + e->batch - 1) / e->batch;
+  const int rows_cta = kGradedThreads / kWarp;
+  const int need = (e->n + rows_cta - 1) / rows_cta;
+  const dim3 pgrid(per_trial < need ? per_trial : need, e->batch);
+  const size_t smem = (size_t)words * sizeof(uint32_t);
+  if (smem > 48 * 1024) {
+    cudaError_t a = cudaFuncSetAttribute(k_graded_pull, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (a != cudaSuccess) return (int)a;
+  }
+  k_graded_pull<<<pgrid, kGradedThreads, smem, st>>>(t_ptr, t_pre, t_val, spikes, e->flags, nz,
+                                                     e->n, words, e->p.w_scale, rec);
   cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) return (int)err;
   k_graded_step<<<grid, kGradedThreads, 0, st>>>(*e, step, spikes, ring, ptr, rec, vstim);

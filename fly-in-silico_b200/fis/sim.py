@@ -325,7 +325,9 @@ class Engine:
             self._t_csr = tuple(torch.from_numpy(a).to(dev) for a in conn.by_post())
             self._fring = torch.zeros((self.batch, self.buf_len, self.n), dtype=torch.float32,
                                       device=dev)
-            self._rec = torch.empty((self.batch, self.n), dtype=torch.float32, device=dev)
+            # the product [B][N], then the nonzero mask [B][ceil(N/32)] words
+            self._rec = torch.empty(self.batch * (self.n + (self.n + 31) // 32),
+                                    dtype=torch.float32, device=dev)
 
     # --- views of the engine's own state ---------------------------------
 

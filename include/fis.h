@@ -314,7 +314,8 @@ int fis_add_rows(const fis_engine* e, int32_t nb, int32_t rows,
  * non-null.  t_ptr int64 [N+1] / t_pre int32 [E] / t_val float [E]: the
  * weights W[post, pre] as CSR by postsynaptic neuron, presynaptic indices
  * ascending within a row.  spikes float [B][N] (read, then written), ring
- * float [B][buf_len][N], rec float [B][N] scratch; 0 <= ptr < buf_len.
+ * float [B][buf_len][N], rec scratch of B*N floats followed by
+ * B*ceil(N/32) 32-bit words; 0 <= ptr < buf_len.
  * Replaces Engine._core's float path (sim.py:863-953) for graded spikes.
  */
 int fis_graded_step(const fis_engine* e, int64_t step, const int64_t* t_ptr,
