@@ -160,3 +160,31 @@ def test_sparse_rows_equal_dense_rows():
     R.reshape(-1)[ra] = rv
     for j, b in enumerate(slots):
         assert np.array_equal(F[b], flags[j]) and np.array_equal(R[b], rates[j]), j
+
+
+def test_sparse_rows_fast_and_sorting_paths_agree():
+    """sparse_rows skips its sort when positions already ascend; the same
+    trials in descending slots (the sorting path) give the same rows, and
+    empty inputs give empty arrays."""
+    from fis.batch import TrialSpec, host_rows, random_specs, sparse_rows
+
+    n = 3000
+    specs = random_specs(n, 5, 11, 50, stim_range=(20, 200), silenced_range=(1, 30))
+    specs.append(TrialSpec(seed=1, steps=10))  # no stimulus, no flags
+    k = len(specs)
+    up = list(range(k))
+    down = list(reversed(range(k)))
+    fa, fb, ra, rv = sparse_rows(specs, n, up)
+    assert np.all(np.diff(fa) > 0) and np.all(np.diff(ra) > 0)
+    flags, rates = host_rows(specs, n)
+    for slots, (a1, b1, a2, v2) in ((up, (fa, fb, ra, rv)), (down, sparse_rows(specs, n, down))):
+        F = np.zeros((k, n), np.uint8)
+        R = np.zeros((k, n), np.float32)
+        F.reshape(-1)[a1] = b1
+        R.reshape(-1)[a2] = v2
+        for j, b in enumerate(slots):
+            assert np.array_equal(F[b], flags[j]) and np.array_equal(R[b], rates[j]), (slots, j)
+    e = sparse_rows([], n, [])
+    assert all(x.size == 0 for x in e)
+    e = sparse_rows([TrialSpec(seed=0, steps=5)], n, [0])
+    assert all(x.size == 0 for x in e)
