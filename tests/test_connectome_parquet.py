@@ -117,3 +117,10 @@ def test_by_post_is_torchs_csr_of_w():
     assert np.array_equal(t_ptr, w.crow_indices().numpy())
     assert np.array_equal(t_pre, w.col_indices().numpy())
     assert np.array_equal(t_val, w.values().numpy())
+
+
+def test_empty_table_gives_neurons_without_edges(tmp_path):
+    f = tmp_path / "empty.parquet"
+    write_table(f, np.zeros(0, np.int64), np.zeros(0, np.int64), np.zeros(0, np.float32))
+    c = C.from_parquet(f, n=17, cache=False)
+    assert c.n == 17 and c.col.size == 0 and np.array_equal(c.row_ptr, np.zeros(18, np.int64))
