@@ -116,22 +116,7 @@ class Connectome:
         an out-of-range index would not fault under a caching allocator, it
         would silently write into a neighbouring tensor.
         """
-        bad = []
-        if self.row_ptr.shape != (self.n + 1,):
-            bad.append("row_ptr has %d entries, expected n+1 = %d"
-                       % (self.row_ptr.shape[0], self.n + 1))
-        elif int(self.row_ptr[0]) != 0 or int(self.row_ptr[-1]) != self.nnz:
-            bad.append("row_ptr spans [%d, %d], expected [0, %d]"
-                       % (int(self.row_ptr[0]), int(self.row_ptr[-1]), self.nnz))
-        elif bool((np.diff(self.row_ptr) < 0).any()):
-            bad.append("row_ptr decreases")
-        if self.cnt.shape != self.col.shape:
-            bad.append("col and cnt lengths differ")
-        if self.nnz:
-            lo, hi = int(self.col.min()), int(self.col.max())
-            if lo < 0 or hi >= self.n:
-                bad.append("postsynaptic indices in [%d, %d], outside [0, %d)"
-                           % (lo, hi, self.n))
+        bad = csr_faults(self.n, self.row_ptr, self.col, self.cnt.shape[0])
         if bad:
             raise ConnectomeError("connectome fails its bounds check:\n  "
                                   + "\n  ".join(bad))
@@ -174,6 +159,34 @@ class Connectome:
         np.cumsum(deg, out=rp[1:])
         return Connectome(self.n, rp, self.col[keep].copy(), self.cnt[keep].copy(),
                           self.seed)
+
+
+def csr_faults(n, row_ptr, col, n_values) -> list:
+    """Every way a CSR of ``n`` rows would send a kernel outside its arrays.
+
+    ``row_ptr`` [n+1] must run from 0 to the edge count without decreasing,
+    ``col`` must hold one index in [0, n) per value.  Returns a list of
+    messages, empty when the arrays are safe to hand to a kernel.
+    """
+    row_ptr = np.asarray(row_ptr)
+    col = np.asarray(col)
+    nnz = int(col.shape[0])
+    faults = []
+    if row_ptr.shape != (n + 1,):
+        faults.append("row_ptr has %d entries, expected n+1 = %d" % (row_ptr.size, n + 1))
+    else:
+        first, last = int(row_ptr[0]), int(row_ptr[-1])
+        if (first, last) != (0, nnz):
+            faults.append("row_ptr spans [%d, %d], expected [0, %d]" % (first, last, nnz))
+        elif np.any(row_ptr[1:] < row_ptr[:-1]):
+            faults.append("row_ptr decreases")
+    if int(n_values) != nnz:
+        faults.append("%d indices but %d values" % (nnz, int(n_values)))
+    if nnz:
+        lo, hi = int(col.min()), int(col.max())
+        if lo < 0 or hi >= n:
+            faults.append("indices in [%d, %d], outside [0, %d)" % (lo, hi, n))
+    return faults
 
 
 def from_weights(weights, n=None) -> Connectome:
