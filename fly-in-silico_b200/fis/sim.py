@@ -91,11 +91,13 @@ class Stimulus:
     name: str = "stim"
 
     def to_dict(self, with_indices=False):
-        d = {"name": self.name, "n": int(len(self.indices)), "rate_hz": self.rate_hz,
-             "t_on_ms": self.t_on_ms, "t_off_ms": self.t_off_ms}
+        """The stimulus as a JSON-ready record (the reference's keys)."""
+        idx = np.asarray(self.indices).ravel()
+        rec = {"name": self.name, "n": int(idx.size)}
+        rec.update((k, getattr(self, k)) for k in ("rate_hz", "t_on_ms", "t_off_ms"))
         if with_indices:
-            d["indices"] = [int(i) for i in self.indices]
-        return d
+            rec["indices"] = idx.astype(np.int64).tolist()
+        return rec
 
 
 @dataclass
@@ -110,66 +112,81 @@ class RunConfig:
     spmv: str | None = None
 
 
-class Result:
-    """Outcome of one run: per-neuron rates plus a neuron x time-bin raster."""
+# Neuron annotation columns a rate table carries when they are present.
+ANNOTATION_COLUMNS = ("root_id", "label", "cell_class", "super_class", "region",
+                      "super_region", "side", "top_nt")
 
-    def __init__(self, counts, bins, config, stimuli, silenced, neurons, timing):
-        self.counts = counts  # int64[N], spikes summed over trials
-        self.bins = bins      # int16[n_bins, N], spikes per bin summed over trials
-        self.config = config
-        self.stimuli = stimuli
-        self.silenced = silenced
-        self.neurons = neurons
-        self.timing = timing
+
+@dataclass
+class Result:
+    """Outcome of one run: per-neuron rates plus a neuron x time-bin raster.
+
+    ``counts`` int64 [N] spikes per neuron summed over trials; ``bins`` int16
+    [n_bins, N] spikes per bin summed over trials (the reference's fields,
+    sim.py:255-321).
+    """
+
+    counts: np.ndarray
+    bins: np.ndarray
+    config: RunConfig
+    stimuli: list
+    silenced: np.ndarray
+    neurons: object
+    timing: dict
 
     @property
     def n_bins(self):
-        return self.bins.shape[0]
+        return int(np.shape(self.bins)[0])
 
     @property
     def rates(self):
         """Firing rate in Hz per neuron, averaged over trials."""
-        return self.counts / (self.config.t_run_s * self.config.n_trials)
+        trial_seconds = self.config.t_run_s * self.config.n_trials
+        return np.asarray(self.counts) / trial_seconds
 
     def active(self, min_rate=0.5):
-        return np.nonzero(self.rates >= min_rate)[0]
+        """Indices of the neurons firing at ``min_rate`` Hz or more."""
+        return np.flatnonzero(self.rates >= min_rate)
 
     def rate_table(self, min_rate=0.5):
+        """Active neurons with their annotations, fastest first."""
         import pandas as pd
 
         idx = self.active(min_rate)
-        if self.neurons is None:
-            return pd.DataFrame({"rate_hz": self.rates[idx], "n_spikes": self.counts[idx]},
-                                index=idx).sort_values("rate_hz", ascending=False)
-        cols = [c for c in ("root_id", "label", "cell_class", "super_class", "region",
-                            "super_region", "side", "top_nt") if c in self.neurons.columns]
-        df = self.neurons.loc[idx, cols].copy()
-        df["rate_hz"] = self.rates[idx]
-        df["n_spikes"] = self.counts[idx]
-        return df.sort_values("rate_hz", ascending=False)
+        table = pd.DataFrame(index=pd.Index(idx))
+        if self.neurons is not None:
+            keep = [c for c in ANNOTATION_COLUMNS if c in self.neurons.columns]
+            table = self.neurons.loc[idx, keep].copy()
+        table["rate_hz"] = self.rates[idx]
+        table["n_spikes"] = np.asarray(self.counts)[idx]
+        return table.sort_values("rate_hz", ascending=False)
 
     def region_timeline(self):
+        """DataFrame region x bin of the mean firing rate in Hz."""
         import pandas as pd
 
-        reg = self.neurons["region"].to_numpy()
-        codes, uniq = pd.factorize(reg)
-        acc = np.zeros((len(uniq), self.n_bins), dtype=np.float64)
-        np.add.at(acc, codes, self.bins.T.astype(np.float64))
-        sizes = np.bincount(codes, minlength=len(uniq)).astype(np.float64)
-        rates = acc / (sizes[:, None] * (self.config.bin_ms / 1000.0) * self.config.n_trials)
-        return pd.DataFrame(rates, index=list(uniq))
+        per_neuron = pd.DataFrame(np.asarray(self.bins, dtype=np.float64).T,
+                                  index=self.neurons["region"].to_numpy())
+        mean_count = per_neuron.groupby(level=0, sort=False).mean()
+        seconds = self.config.bin_ms / 1000.0 * self.config.n_trials
+        return mean_count / seconds
 
     def meta(self, with_indices=False):
+        """The run record written to meta.json (the reference's keys)."""
+        cfg = asdict(self.config)
+        params = cfg.pop("params")
+        sil = np.asarray(self.silenced).astype(np.int64)
+        rates = self.rates
         return {
-            "config": {k: v for k, v in asdict(self.config).items() if k != "params"},
-            "params": self.config.params,
+            "config": cfg,
+            "params": params,
             "stimuli": [s.to_dict(with_indices) for s in self.stimuli],
-            "silenced": [int(i) for i in self.silenced] if with_indices else None,
-            "n_silenced": int(len(self.silenced)),
+            "silenced": sil.tolist() if with_indices else None,
+            "n_silenced": int(sil.size),
             "timing": self.timing,
-            "n_neurons": int(len(self.counts)),
-            "n_active": int((self.rates >= 0.5).sum()),
-            "total_spikes": int(self.counts.sum()),
+            "n_neurons": int(np.size(self.counts)),
+            "n_active": int(np.count_nonzero(rates >= 0.5)),
+            "total_spikes": int(np.sum(self.counts)),
         }
 
 
@@ -727,18 +744,15 @@ class Engine:
         return done
 
 
-def build_engine(weights=None, neurons=None, silenced=None, params=None, device=None,
-                 batch=1, seed=0, no_refractory=None, graphs=True, spmv=None,
-                 allow_inexact=False, group=None, ring=None, graded=False):
-    """Return a ready :class:`Engine` (sim.py:956-987).
+def connectome_of(weights=None):
+    """The connectome a run or an engine is built on.
 
     ``weights`` is the reference's sparse ``W[post, pre]`` or a
     :class:`fis.connectome.Connectome`.  The reference loads FlyWire from its
-    data directory when ``weights`` is None (data.py:229-259); here that
-    directory is named by the environment variable ``FIS_FLYWIRE_DATA`` (the
-    upstream ``data`` folder with its connectivity parquet and completeness
-    CSV), and without it ``weights`` is required.  ``graded=True`` builds the
-    graded-spike mode of :class:`Engine`.
+    data directory when ``weights`` is None (sim.py:981-982, data.py:229-259);
+    here that directory is named by the environment variable
+    ``FIS_FLYWIRE_DATA`` (the upstream ``data`` folder with its connectivity
+    parquet and completeness CSV), and without it ``weights`` is required.
     """
     if weights is None:
         data = os.environ.get("FIS_FLYWIRE_DATA")
@@ -747,8 +761,20 @@ def build_engine(weights=None, neurons=None, silenced=None, params=None, device=
                 "no connectome given: pass weights= (torch sparse W[post, pre] of synapse "
                 "counts, or fis.connectome.Connectome), or set FIS_FLYWIRE_DATA to the "
                 "upstream data folder")
-        weights = C.from_upstream(data)
-    conn = weights if isinstance(weights, C.Connectome) else C.from_weights(weights)
+        return C.from_upstream(data)
+    return weights if isinstance(weights, C.Connectome) else C.from_weights(weights)
+
+
+def build_engine(weights=None, neurons=None, silenced=None, params=None, device=None,
+                 batch=1, seed=0, no_refractory=None, graphs=True, spmv=None,
+                 allow_inexact=False, group=None, ring=None, graded=False):
+    """Return a ready :class:`Engine` (sim.py:956-987).
+
+    ``weights`` as :func:`connectome_of` takes it (None: the FlyWire folder
+    named by ``FIS_FLYWIRE_DATA``).  ``graded=True`` builds the graded-spike
+    mode of :class:`Engine`.
+    """
+    conn = connectome_of(weights)
     n = len(neurons) if neurons is not None else conn.n
     sil = np.asarray(silenced if silenced is not None else [], dtype=np.int64)
     conn = conn.without(sil)
@@ -780,13 +806,14 @@ def run(stimuli, silenced=None, config: RunConfig | None = None, neurons=None, w
 
     Binning happens on the device: each spike adds one to its (bin, neuron)
     counter inside the update kernel, so the host reads back only at bin
-    boundaries where ``on_bin`` or ``should_stop`` ask for it.
+    boundaries where ``on_bin`` or ``should_stop`` ask for it.  ``weights``
+    as :func:`connectome_of` takes it.  The steps run in fused blocks of up
+    to 20 without CUDA graphs whatever ``config.speed`` says, so the
+    timing record states ``"graphs": False``.
     """
     config = config or RunConfig()
     silenced = np.asarray([] if silenced is None else silenced, dtype=np.int64)
-    if weights is None:
-        raise FileNotFoundError("no connectome given: pass weights=")
-    conn = weights if isinstance(weights, C.Connectome) else C.from_weights(weights)
+    conn = connectome_of(weights)
     n = len(neurons) if neurons is not None else conn.n
     device = config.device or "cuda"
     t0 = time.perf_counter()
@@ -868,41 +895,56 @@ def run(stimuli, silenced=None, config: RunConfig | None = None, neurons=None, w
                   silenced, neurons, timing)
 
 
+# The saved-run format (sim.py:1120-1174): meta.json (Result.meta with the
+# indices), rates.parquet (the rate table of active neurons, indexed by
+# neuron) and bins.npz (the active neurons' columns of the raster).
+META_FILE, RATES_FILE, BINS_FILE = "meta.json", "rates.parquet", "bins.npz"
+
+
 def save(result: Result, out_dir: Path, min_rate=0.5):
-    """Write meta.json, rates.parquet and bins.npz (sim.py:1120-1140)."""
-    out_dir = Path(out_dir)
-    out_dir.mkdir(parents=True, exist_ok=True)
-    (out_dir / "meta.json").write_text(
-        json.dumps(result.meta(with_indices=True), ensure_ascii=False, indent=2),
-        encoding="utf-8")
-    result.rate_table(min_rate).to_parquet(out_dir / "rates.parquet")
-    keep = result.active(min_rate)
-    np.savez_compressed(out_dir / "bins.npz", neuron_idx=keep.astype(np.int32),
-                        bins=result.bins[:, keep].astype(np.int16),
-                        bin_ms=np.float32(result.config.bin_ms),
-                        t0_ms=np.float32((result.timing or {}).get("запись с, мс", 0.0)))
-    return out_dir
+    """Write a run directory (meta.json, rates.parquet, bins.npz); returns it."""
+    out = Path(out_dir)
+    out.mkdir(parents=True, exist_ok=True)
+    record = json.dumps(result.meta(with_indices=True), ensure_ascii=False, indent=2)
+    (out / META_FILE).write_text(record, encoding="utf-8")
+    result.rate_table(min_rate).to_parquet(out / RATES_FILE)
+    cols = result.active(min_rate)
+    # t0_ms: model time of the first raster row (a windowed recording
+    # states it in its timing record; an ordinary run starts at 0)
+    t0 = (result.timing or {}).get("запись с, мс", 0.0)
+    raster = np.asarray(result.bins)[:, cols].astype(np.int16)
+    np.savez_compressed(out / BINS_FILE, neuron_idx=cols.astype(np.int32), bins=raster,
+                        bin_ms=np.float32(result.config.bin_ms), t0_ms=np.float32(t0))
+    return out
 
 
 def load(out_dir, neurons=None, n=None) -> Result:
-    """Rebuild a :class:`Result` from a saved run directory (sim.py:1143-1174)."""
+    """Rebuild a :class:`Result` from a run directory written by :func:`save`.
+
+    The neuron count comes from ``neurons``, else ``n``, else the record's
+    ``n_neurons``; neurons absent from the saved tables read as silent.
+    """
     import pandas as pd
 
-    out_dir = Path(out_dir)
-    meta = json.loads((out_dir / "meta.json").read_text(encoding="utf-8"))
-    n = len(neurons) if neurons is not None else int(n or meta["n_neurons"])
-    rates_df = pd.read_parquet(out_dir / "rates.parquet")
-    counts = np.zeros(n, dtype=np.int64)
-    counts[rates_df.index.to_numpy()] = rates_df["n_spikes"].to_numpy()
-    z = np.load(out_dir / "bins.npz")
-    bins = np.zeros((z["bins"].shape[0], n), dtype=np.int16)
-    bins[:, z["neuron_idx"]] = z["bins"]
-    cfg = RunConfig(**meta["config"], params=meta["params"])
-    stimuli = [Stimulus(indices=np.asarray(s.get("indices", []), dtype=np.int64),
-                        rate_hz=s["rate_hz"], t_on_ms=s["t_on_ms"], t_off_ms=s["t_off_ms"],
-                        name=s["name"]) for s in meta["stimuli"]]
+    where = Path(out_dir)
+    meta = json.loads((where / META_FILE).read_text(encoding="utf-8"))
+    size = len(neurons) if neurons is not None else int(n or meta["n_neurons"])
+    table = pd.read_parquet(where / RATES_FILE)
+    counts = np.zeros(size, dtype=np.int64)
+    np.put(counts, table.index.to_numpy(), table["n_spikes"].to_numpy())
+    with np.load(where / BINS_FILE) as z:
+        cols, part = z["neuron_idx"], z["bins"]
+    bins = np.zeros((part.shape[0], size), dtype=np.int16)
+    bins[:, cols] = part
+    config = RunConfig(params=meta["params"], **meta["config"])
+
+    def stimulus(rec):
+        idx = np.asarray(rec.get("indices", []), dtype=np.int64)
+        return Stimulus(idx, **{k: rec[k] for k in ("rate_hz", "t_on_ms", "t_off_ms", "name")})
+
     silenced = np.asarray(meta.get("silenced") or [], dtype=np.int64)
-    return Result(counts, bins, cfg, stimuli, silenced, neurons, meta["timing"])
+    return Result(counts, bins, config, [stimulus(r) for r in meta["stimuli"]], silenced,
+                  neurons, meta["timing"])
 
 
 __all__ = ["MODEL_PARAMS", "DT", "FAST", "REFERENCE", "SPMV_CSR", "SPMV_EVENT",
