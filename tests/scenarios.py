@@ -117,3 +117,37 @@ def graded_spikes(sc, step):
     b = np.arange(sc["batch"])[:, None]
     vals = ((j * 7 + step * 3 + b * 5) % 17) / 17.0 * 0.9
     return idx, vals.astype(np.float32)
+
+
+# sim.run through the experiment API (sim.py:990-1117): three stimuli whose
+# windows switch on and off mid-bin and on a bin edge, per-trial Philox
+# streams, silencing through the reference's own build path, a run length
+# that leaves the last bin partial, and a second run that a should_stop
+# callback cuts after bin ``stop_after_bin``.
+RUN_SCENARIOS = {
+    "run_b2": dict(n=2500, e=2500 * 110, conn_seed=21, batch=2, seed=31, t_run_s=0.0473,
+                   bin_ms=5.0, silenced_k=40, silenced_seed=44, stop_after_bin=5,
+                   stimuli=[dict(name="a", k=300, seed=41, rate_hz=210.0, t_on_ms=0.0,
+                                 t_off_ms=20.0),
+                            dict(name="b", k=250, seed=42, rate_hz=120.0, t_on_ms=12.3,
+                                 t_off_ms=None),
+                            dict(name="c", k=200, seed=43, rate_hz=90.0, t_on_ms=7.77,
+                                 t_off_ms=31.4)]),
+}
+
+
+def run_stimuli(sc):
+    """``(name, indices, rate_hz, t_on_ms, t_off_ms)`` of a run scenario."""
+    out = []
+    for s in sc["stimuli"]:
+        rng = np.random.default_rng(s["seed"])
+        idx = np.sort(rng.choice(sc["n"], size=s["k"], replace=False)).astype(np.int64)
+        out.append((s["name"], idx, s["rate_hz"], s["t_on_ms"], s["t_off_ms"]))
+    return out
+
+
+# Reference snapshots (sim.py:780-814) taken mid-run, for restoring a state
+# the reference wrote into this engine: scenario -> step of the snapshot.
+# batch3_masks at 320 is inside the window where all four masks are set
+# (hold included, so v_hold is not zero); silenced_b2 at 150 is mid-run.
+SNAPSHOTS = {"batch3_masks": 320, "silenced_b2": 150}

@@ -188,3 +188,78 @@ def test_sparse_rows_fast_and_sorting_paths_agree():
     assert all(x.size == 0 for x in e)
     e = sparse_rows([TrialSpec(seed=0, steps=5)], n, [0])
     assert all(x.size == 0 for x in e)
+
+
+def test_exactness_record_and_transpose():
+    """evspmv.exactness: the reference's record (keys and verdict) computed
+    from the CSR arrays; Events' transposition lists each presynaptic row with
+    its postsynaptic indices ascending."""
+    import torch
+
+    from fis import evspmv
+
+    c = C.synthetic(n=700, e=700 * 40, seed=4, cache=False)
+    w = c.to_torch_weights().to_sparse_csr()
+    rec = evspmv.exactness(w)
+    want = float(c.in_abs_sum().max())
+    assert rec["макс сумма модулей по строке"] == want
+    assert rec["значения целые"] and rec["годится"]
+    assert rec["мин значение"] == float(c.cnt.min()) and rec["макс значение"] == float(c.cnt.max())
+    assert rec["запас"] == round((1 << 24) / want, 1)
+    frac = torch.sparse_csr_tensor(w.crow_indices(), w.col_indices(), w.values() + 0.25,
+                                   size=w.shape)
+    bad = evspmv.exactness(frac)
+    assert not bad["значения целые"] and not bad["годится"] and bad["макс нецелая часть"] == 0.25
+    n, _, rp, col, val = evspmv._csr_arrays(w)
+    t_ptr, t_post, t_val = evspmv._by_pre(n, rp, col, val)
+    assert t_ptr.dtype == rp.dtype and t_post.dtype == col.dtype
+    assert np.array_equal(t_ptr, c.row_ptr) and np.array_equal(t_post, c.col)
+    assert np.array_equal(t_val, c.cnt.astype(np.float32))
+
+
+def test_csr_faults_name_each_fault():
+    rp = np.array([0, 2, 3], dtype=np.int64)
+    assert C.csr_faults(2, rp, np.array([1, 0, 1]), 3) == []
+    assert any("outside" in f for f in C.csr_faults(2, rp, np.array([1, 0, 2]), 3))
+    assert any("n+1" in f for f in C.csr_faults(2, np.array([0, 3, 2, 3]), np.zeros(3), 3))
+    assert any("decreases" in f for f in C.csr_faults(2, np.array([0, 4, 3]), np.zeros(3), 3))
+    assert any("values" in f for f in C.csr_faults(2, rp, np.array([1, 0, 1]), 4))
+
+
+def test_result_save_load_round_trip(tmp_path):
+    """save() writes the reference's three files; load() rebuilds the same
+    counts, bins, config, stimuli and silencing."""
+    import pandas as pd
+
+    from fis import sim
+
+    rng = np.random.default_rng(5)
+    n = 400
+    bins = rng.integers(0, 3, size=(7, n)).astype(np.int16)
+    bins[:, ::3] = 0
+    neurons = pd.DataFrame({"root_id": np.arange(n) + 10 ** 9,
+                            "region": np.array(["AL", "MB"])[np.arange(n) % 2]})
+    cfg = sim.RunConfig(t_run_s=0.07, bin_ms=10.0, n_trials=2, seed=3)
+    stims = [sim.Stimulus(np.array([5, 9, 11]), 150.0, 1.0, None, "s1"),
+             sim.Stimulus(np.array([2]), 90.0, 0.0, 30.0, "s2")]
+    res = sim.Result(bins.sum(0).astype(np.int64), bins, cfg, stims, np.array([4, 8]), neurons,
+                     {"steps": 700, "sim_s": 0.1})
+    meta = res.meta(with_indices=True)
+    assert meta["stimuli"][0] == {"name": "s1", "n": 3, "rate_hz": 150.0, "t_on_ms": 1.0,
+                                  "t_off_ms": None, "indices": [5, 9, 11]}
+    assert meta["silenced"] == [4, 8] and res.meta()["silenced"] is None
+    assert meta["n_active"] == int((res.counts / (0.07 * 2) >= 0.5).sum())
+    out = sim.save(res, tmp_path / "run")
+    assert sorted(p.name for p in out.iterdir()) == ["bins.npz", "meta.json", "rates.parquet"]
+    back = sim.load(out, neurons=neurons)
+    assert np.array_equal(back.counts, res.counts)
+    assert np.array_equal(back.bins, res.bins)
+    assert back.config == cfg
+    assert [s.to_dict(True) for s in back.stimuli] == [s.to_dict(True) for s in stims]
+    assert list(back.silenced) == [4, 8] and back.timing == res.timing
+    table = res.rate_table()
+    assert list(table.columns) == ["root_id", "region", "rate_hz", "n_spikes"]
+    assert table["rate_hz"].is_monotonic_decreasing
+    tl = res.region_timeline()
+    want = bins[:, ::2].mean(1) / (0.01 * 2)
+    assert np.allclose(tl.loc["AL"].to_numpy(), want)

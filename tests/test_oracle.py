@@ -165,3 +165,90 @@ def test_oracle_catches_planted_mistakes(golden):
     assert diverges(one_count) is not None
     assert diverges(ones_mask) is not None
     assert diverges(ring_shift) is not None
+
+
+def oracle_sim_run(name, stop_after=None):
+    """The experiment driver of sim.py:990-1083 over the oracle's step: the
+    rate schedule, int16 bins summed over trials, the on_bin stream and the
+    should_stop cut, written out here from the reference's description."""
+    sc = S.RUN_SCENARIOS[name]
+    conn = S.connectome(sc).without(S.silenced(sc))
+    stims = S.run_stimuli(sc)
+    steps = int(round(sc["t_run_s"] * 1000.0 / O.DT))
+    bin_steps = max(1, int(round(sc["bin_ms"] / O.DT)))
+    n_bins = -(-steps // bin_steps)
+    switches = []
+    for _, idx, rate, on, off in stims:
+        switches.append((int(round(on / O.DT)), idx, rate))
+        stop = steps if off is None else int(round(off / O.DT))
+        if stop < steps:
+            switches.append((stop, idx, 0.0))
+    switches.sort(key=lambda e: e[0])
+    o = O.Oracle.from_connectome(conn, batch=sc["batch"], seed=sc["seed"],
+                                 no_refractory=np.concatenate([s[1] for s in switches]))
+    bins = np.zeros((n_bins, sc["n"]), dtype=np.int64)
+    calls = []
+    polls = 0
+    for step in range(steps):
+        for at, idx, rate in switches:
+            if at == step:
+                o.rates[:, idx] = rate
+        vs = O.drive_tape(o.rates, o.seeds, o.streams, np.full(sc["batch"], step))
+        o.core(vs, mode=O.Oracle.CSRMV)
+        b = step // bin_steps
+        bins[b] += o.spikes.sum(0).astype(np.int64)
+        if (step + 1) % bin_steps == 0 or step == steps - 1:
+            calls.append((b, (step + 1) * O.DT, bins[b].astype(np.int16)))
+            polls += 1
+            if stop_after is not None and polls > stop_after:
+                steps = step + 1
+                break
+    return bins, calls, steps
+
+
+@pytest.mark.parametrize("tag", ["full", "stop"])
+def test_oracle_sim_run_matches_reference(tag, golden):
+    """The run golden (the reference's own sim.run on the tape) against the
+    oracle stepping the same schedule: pins the fixture's drive convention
+    (one Philox stream per trial, keyed by the run seed, own step = call)."""
+    z = golden("run_b2")
+    sc = S.RUN_SCENARIOS["run_b2"]
+    bins, calls, steps = oracle_sim_run("run_b2", sc["stop_after_bin"] if tag == "stop" else None)
+    assert steps == int(z[tag + "_steps"])
+    assert np.array_equal(bins.astype(np.int16), z[tag + "_bins"])
+    assert np.array_equal(bins.sum(0), z[tag + "_counts"])
+    assert [c[0] for c in calls] == list(z[tag + "_onbin_b"])
+    assert [c[1] for c in calls] == list(z[tag + "_onbin_t"])
+    assert np.array_equal(np.stack([c[2] for c in calls]), z[tag + "_onbin_counts"])
+
+
+@pytest.mark.parametrize("name", sorted(S.SNAPSHOTS))
+def test_reference_snapshot_continues_in_oracle(name, golden):
+    """The reference's mid-run snapshot, put into the oracle's state, continues
+    to the reference's final raster and state."""
+    z = golden(name)
+    at = S.SNAPSHOTS[name]
+    snap = golden("%s_snap%d" % (name, at))
+    sc = S.SCENARIOS[name]
+    conn = S.connectome(sc)
+    sil = S.silenced(sc)
+    if sil.size:
+        conn = conn.without(sil)
+    o = O.Oracle.from_connectome(conn, batch=sc["batch"], params_dict=sc["params"],
+                                 no_refractory=S.driven(sc), seed=sc["seed"])
+    o.rates[:] = S.rates_matrix(sc)
+    for key in ("v", "conductance", "spikes", "refrac", "delay_buffer", "m_fire", "m_out",
+                "m_in", "m_hold", "v_hold"):
+        getattr(o, key)[...] = snap[key]
+    o.ptr[0] = int(snap["ptr"])
+    plan = dict(sc["plan"])
+    idx = S.busy(sc)
+    rows = []
+    for step in range(at, sc["steps"]):
+        if step in plan:
+            o.set_masks(**S.mask_call(plan[step], idx))
+        vs = O.drive_tape(o.rates, o.seeds, o.streams, np.full(sc["batch"], step), sc["params"])
+        o.core(vs, mode=O.Oracle.EVENT)
+        rows.append(np.packbits(o.spikes != 0, axis=1, bitorder="little"))
+    assert np.array_equal(np.stack(rows), z["raster_bits"][at:])
+    assert np.array_equal(o.v, z["v"]) and np.array_equal(o.delay_buffer, z["ring"])
