@@ -812,8 +812,13 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
   unsigned arrived = 0;
   if (bump && threadIdx.x == 0) arrived = atomicAdd(E.done, 1u) + 1u;
   if (failed) {
+    // The staged lines were neither consumed nor returned to empty: the
+    // host must refill the ring before it is used again.  A second wait
+    // that also runs out leaves copies that may still write this CTA's
+    // shared memory after it ends: FIS_ERR_STAGE_LOST, fatal for the context.
     if (threadIdx.x == 0) atomicOr(E.done + 1, (uint32_t)FIS_ERR_STAGE);
-    if (!staged_ok) mbar_wait(&sbar, 0, polls);
+    if (!staged_ok && !mbar_wait(&sbar, 0, polls))
+      atomicOr(E.done + 1, (uint32_t)FIS_ERR_STAGE_LOST);
   } else {
   // The staged lines are in shared memory: warp 0 returns them to empty in
   // the ring with one bulk store each, so the scratch ring needs no clearing
@@ -1136,17 +1141,24 @@ int fis_check(const fis_engine* e) {
   return FIS_OK;
 }
 
-static int check_block(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps,
-                       const int32_t* ring) {
+// Everything fis_block checks except the ring pointer itself.
+static int check_block_shape(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps) {
   int rc = fis_check(e);
   if (rc) return rc;
   if ((rc = check_range(e, b0, nb))) return rc;
-  if (!ring) return FIS_E_ARG;
   if (k_steps < 1 || k_steps > FIS_MAX_BLOCK || k_steps > e->p.lag) return FIS_E_BOUNDS;
   if (e->vstim && k_steps != 1) return FIS_E_BOUNDS;
   if ((k_steps + 1) * nb + 1 > kMaxLists) return FIS_E_BOUNDS;
   const int64_t rows = (int64_t)nb * ring_row(e->n);
   if (rows * FIS_MAX_BLOCK > 0x7FFFFFFFLL) return FIS_E_BOUNDS;
+  return FIS_OK;
+}
+
+static int check_block(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps,
+                       const int32_t* ring) {
+  const int rc = check_block_shape(e, b0, nb, k_steps);
+  if (rc) return rc;
+  if (!ring) return FIS_E_ARG;
   if (((uintptr_t)ring & 15u) != 0) return FIS_E_ALIGN;
   return FIS_OK;
 }
@@ -1515,9 +1527,10 @@ int noalloc_ring(int32_t** out) {
 
 extern "C" int fis_block_noalloc(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps,
                                  float* spikes_out, int32_t last_group, void* stream) {
-  int rc = fis_check(e);
+  // Every argument check fis_block makes, before the array is touched: a
+  // refused call launches nothing.
+  int rc = check_block_shape(e, b0, nb, k_steps);
   if (rc) return rc;
-  if (nb < 1 || k_steps < 1) return FIS_E_BOUNDS;
   const int64_t need = ring_words(e, k_steps, nb);
   if (need > (int64_t)FIS_NOALLOC_RING_INTS) return FIS_E_BOUNDS;
   int32_t* ring = nullptr;

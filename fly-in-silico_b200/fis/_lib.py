@@ -29,6 +29,10 @@ FIS_FL_HOLD = 1 << 3
 FIS_FL_NOREFRAC = 1 << 4
 FIS_FL_SILENCED = 1 << 5
 
+# device error bits in done[1] (FIS_ERR_*)
+FIS_ERR_STAGE = 1 << 0
+FIS_ERR_STAGE_LOST = 1 << 1
+
 STATUS = {0: "ok", -1: "FIS_E_ARG (null pointer or size out of range)",
           -2: "FIS_E_BOUNDS (trial range, block length or slot out of range)",
           -3: "FIS_E_ALIGN (array not 16-byte aligned)"}

@@ -81,6 +81,10 @@ def _ptr(t):
 class Core:
     """B trial slots, their state on the device, and the block launcher."""
 
+    # an empty word of the paired int16 ring: the biased zero 0x8000 in both
+    # halves (0x80008000 as int32); the int32 ring's empty value is 0
+    RING_EMPTY16 = -0x7FFF8000
+
     def __init__(self, conn: Connectome, batch: int, params=None, device="cuda",
                  group=None, chunk=None, max_block=_lib.FIS_MAX_BLOCK, ring=None,
                  overlap=True, raster=True):
@@ -213,12 +217,28 @@ class Core:
         return host
 
     def raise_errors(self, err):
-        """Raise for error bits ``err`` (an int, or a word from ``errors_async``)."""
+        """Raise for error bits ``err`` (an int, or a word from ``errors_async``).
+
+        A CTA that gave up waiting for its staged input left its lines of the
+        scratch ring as the scatter wrote them, so the rings are refilled with
+        their empty value before the error is raised: the core stays usable
+        for a fresh run.  If a CTA also gave up on the copies still in flight
+        (FIS_ERR_STAGE_LOST), the CUDA context cannot be trusted any more.
+        """
         err = int(err[0]) if torch.is_tensor(err) else int(err)
-        if err:
-            self.done[1].zero_()
-            raise RuntimeError("the device reported error bits 0x%x (FIS_ERR_STAGE = 1: "
-                               "a block's staged input did not arrive)" % err)
+        if not err:
+            return
+        self.done[1].zero_()
+        self._empty_rings()
+        if err & _lib.FIS_ERR_STAGE_LOST:
+            raise RuntimeError("the device reported error bits 0x%x: copies into a CTA's "
+                               "shared memory outlived it (FIS_ERR_STAGE_LOST); this CUDA "
+                               "context is not safe to use further" % err)
+        raise RuntimeError("the device reported error bits 0x%x (FIS_ERR_STAGE = 1: "
+                           "a block's staged input did not arrive)" % err)
+
+    def _empty_rings(self):
+        self.ring2.fill_(self.RING_EMPTY16 if self.ring16 else 0)
 
     def set_clock(self, step):
         """Set the device step counter (and its slot indices) and the host mirror."""
@@ -246,10 +266,9 @@ class Core:
         self.ring_row = int(self.lib.fis_ring_row(self.n))
         shape = (2 if self.overlap else 1, self.max_block, self.ring_rows(self.group),
                  self.ring_row)
-        # empty: 0 counts, or the biased zero 0x8000 in both halves of a word
-        empty = -0x7FFF8000 if self.ring16 else 0   # 0x80008000 as int32
         with torch.cuda.device(self.device):
-            self.ring2 = torch.full(shape, empty, dtype=torch.int32, device=self.device)
+            self.ring2 = torch.full(shape, self.RING_EMPTY16 if self.ring16 else 0,
+                                    dtype=torch.int32, device=self.device)
         self.ring = self.ring2[0]
 
     def set_recordings(self, bufs):
@@ -295,7 +314,8 @@ class Core:
 
     # --- stepping ------------------------------------------------------------
 
-    def block(self, k, spikes_out=None, stream=None, timer=None, rows=None):
+    def block(self, k, spikes_out=None, stream=None, timer=None, rows=None,
+              scatter_timer=None):
         """Advance every slot by ``k`` steps (1 <= k <= max_block).
 
         ``rows``: launch only the trial groups covering slots [0, rows); the
@@ -303,7 +323,8 @@ class Core:
         is launched again later is re-initialised first, see reset_slots).
         ``timer`` (optional) is called as ``timer(stream, True)`` right before
         and ``timer(stream, False)`` right after each update launch, so a caller
-        can bracket the dominant kernel with CUDA events.
+        can bracket the dominant kernel with CUDA events; ``scatter_timer`` the
+        same around each phase-A launch (scatter and Poisson drive).
         """
         k = int(k)
         if not 1 <= k <= self.max_block:
@@ -318,9 +339,13 @@ class Core:
             if self.pending is not None:
                 self._apply_pending(g0, nb, k, st)
             ring = ctypes.c_void_p(self.ring.data_ptr())
+            if scatter_timer is not None:
+                scatter_timer(st, True)
             rc = self.lib.fis_scatter(ctypes.byref(self.desc), g0, nb, k, ring,
                                       ctypes.c_void_p(st))
             _lib.check(rc, "fis_scatter")
+            if scatter_timer is not None:
+                scatter_timer(st, False)
             if timer is not None:
                 timer(st, True)
             rc = self.lib.fis_update(ctypes.byref(self.desc), g0, nb, k, ring, sp,

@@ -40,9 +40,17 @@ enum {
   FIS_E_ALIGN = -3    /* an array is not 16-byte aligned */
 };
 
-/* Error bits the device sets in done[1].  A CTA whose staged input did not
- * arrive within wait_polls skipped its update; the run is then invalid. */
-enum { FIS_ERR_STAGE = 1u << 0 };
+/* Error bits the device sets in done[1].
+ * FIS_ERR_STAGE: a CTA whose staged input did not arrive within wait_polls
+ *   skipped its update; the run is then invalid, and the CTA left its lines
+ *   of the scratch ring as the scatter wrote them, so the caller must refill
+ *   the whole ring with its empty value (0, or 0x80008000 per word with
+ *   ring16) before passing it to another call.
+ * FIS_ERR_STAGE_LOST: a CTA's second bounded wait, for copies still in
+ *   flight after the first ran out, ran out as well; those copies may have
+ *   written shared memory after the CTA ended.  Treat the CUDA context as
+ *   unusable (destroy it, or end the process). */
+enum { FIS_ERR_STAGE = 1u << 0, FIS_ERR_STAGE_LOST = 1u << 1 };
 
 /* Per-neuron flag bits, one byte per (trial, neuron). */
 enum {
@@ -335,7 +343,8 @@ int fis_ring_row(int32_t n);
  * FIS_E_BOUNDS.  Every GPU that loads the library keeps the array until
  * exit; calls overlapping on the GPU race on it; each call clears what it
  * uses; the first call on a device looks up the array's address and should
- * come before any stream capture.
+ * come before any stream capture.  Arguments are checked as fis_block
+ * checks them before anything is launched.
  */
 #define FIS_NOALLOC_RING_INTS (3 << 20)
 int fis_block_noalloc(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps,

@@ -81,3 +81,26 @@ def test_noalloc_refuses_blocks_larger_than_its_array(ring, trials):
     rc = lib.fis_block_noalloc(ctypes.byref(core.desc), 0, trials, 20, None, 1,
                                ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
     assert rc == -2  # FIS_E_BOUNDS, nothing launched
+
+
+def test_noalloc_checks_arguments_before_touching_its_array():
+    """A refused call returns fis_block's status for the same arguments (block
+    longer than the delay allows, trial range outside the batch, an external
+    drive over a multi-step block), checked before the array is cleared."""
+    import fis._lib as L
+    import fis.connectome as C
+    from fis.engine import Core
+
+    conn = C.synthetic(n=3000, e=3000 * 100, seed=2)
+    core = Core(conn, 2, group=2)
+    lib = L.load()
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for b0, nb, k in ((0, 1, L.FIS_MAX_BLOCK + 1), (0, 1, 0), (1, 2, 20), (-1, 1, 20),
+                      (0, 0, 20)):
+        rc = lib.fis_block_noalloc(ctypes.byref(core.desc), b0, nb, k, None, 1, stream)
+        assert rc == -2, (b0, nb, k)
+    vs = torch.zeros((2, conn.n), device=core.device)
+    core.desc.vstim = vs.data_ptr()
+    assert lib.fis_block_noalloc(ctypes.byref(core.desc), 0, 1, 2, None, 1, stream) == -2
+    core.desc.vstim = None
+    torch.cuda.synchronize()
