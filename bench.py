@@ -40,17 +40,22 @@ WORKLOAD = ("batched 64 trials x 10,000 steps (1 s), N=138,639, E=15,091,983 syn
 SPEC_SEED = 2024
 CONN_SEED = 0
 # Update-kernel DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum)
-# per trial-neuron and block, from the ncu capture summarised in
-# profiles/k_update_batched64.md (187.0 MB for one launch of 16 trials x
-# 138,639 neurons x 20 steps at steady activity; ncu flushes caches between
-# replay passes, so this counts the L2-resident scratch ring as cold reads and
-# its clearing as DRAM writes, an upper bound).  Scaled to the bench's launch
-# size by the neurons it processes.
+# per trial-neuron and block, from one ncu capture of a 16-trial, 20-step
+# launch at steady activity (187.0 MB; ncu flushes caches between replay
+# passes, so the scratch ring counts as cold reads and its clearing as DRAM
+# writes).  Scaled to the bench's launch size by the neurons it processes.
 NCU_TRAFFIC_PER_NEURON_BLOCK = 187.04e6 / (16 * 138_639)
-# Algorithmic HBM bytes of the update per trial-neuron and block: state
-# v, g, refrac read and written (24), flags (1), rates (4), kick steps (4),
-# and the previous and last step's raster bits (2/8).
-UPDATE_BYTES_PER_NEURON_BLOCK = 24 + 1 + 4 + 4 + 2 / 8
+
+
+def update_bytes_per_neuron_block(core):
+    """Algorithmic bytes the update moves per trial-neuron and block of K
+    steps: state v, g, refrac read and written (24), flags (1), rates (4),
+    kick steps (4), the previous and last step's raster bits (2/8), and the
+    scratch ring -- each of the K slots staged into shared memory and stored
+    back empty (2 + 2 bytes a slot with the paired int16 ring, 4 + 4 with
+    int32)."""
+    ring = core.max_block * (4 if core.ring16 else 8)
+    return 24 + 1 + 4 + 4 + 2 / 8 + ring
 
 
 def parse():
@@ -96,29 +101,138 @@ def uneven_run(conn, group):
                              "in place until the longest ends"}
 
 
-def serving_run(conn, group, plain_value):
-    """Open-loop stream: Poisson arrivals at 2 req/s, 1-64 trials, 1,000-50,000 steps."""
+SERVING_RATES_HZ = (2.0, 10.0, 50.0)
+
+
+def serving_run(conn, group, plain_value, rates=SERVING_RATES_HZ, count=100):
+    """Open-loop streams of ``count`` requests at each Poisson arrival rate:
+    1-64 trials and 1,000-50,000 steps per request, 10 ms bins.  Latency is
+    arrival to result on the host; it splits into the admission wait (queued
+    until slots and recording memory are free) and the service time."""
     import torch
 
     from fis.serve import Server, poisson_requests
 
-    reqs = poisson_requests(conn.n, SPEC_SEED + 9, 2.0, 12, trials=(1, 64),
-                            steps=(1000, 50000), bin_steps=100)
+    lines = []
     srv = Server(conn, capacity=256, group=group)
-    t0 = time.perf_counter()
-    replies = srv.run(reqs, realtime=True)
-    wall = time.perf_counter() - t0
-    lat = Server.latency_stats(replies)
-    units = sum(r.trial_steps for r in replies) * conn.n
-    out = {"requests": len(replies), "arrival_rate_hz": 2.0, "p50_s": lat["p50_s"],
-           "p99_s": lat["p99_s"], "mean_s": lat["mean_s"],
-           "throughput": units / wall, "unit": "neuron-steps/s", "wall_s": wall,
-           "serial_plain_s": units / plain_value if plain_value else None,
-           "how": "Poisson arrivals, admission by free slots and recording memory, "
-                  "continuous batching into 256 slots, 10 ms bins per request"}
+    for j, hz in enumerate(rates):
+        reqs = poisson_requests(conn.n, SPEC_SEED + 9 + j, hz, count, trials=(1, 64),
+                                steps=(1000, 50000), bin_steps=100)
+        srv.replies = []
+        t0 = time.perf_counter()
+        replies = srv.run(reqs, realtime=True)
+        wall = time.perf_counter() - t0
+        srv.core.check_errors()
+        lat = Server.latency_stats(replies)
+        units = sum(r.trial_steps for r in replies) * conn.n
+        lines.append({"arrival_rate_hz": hz, "requests": len(replies), **lat,
+                      "throughput": units / wall, "unit": "neuron-steps/s", "wall_s": wall,
+                      "serial_plain_s": units / plain_value if plain_value else None})
     del srv
     torch.cuda.empty_cache()
+    return {"rates": lines,
+            "how": "Poisson arrivals, %d requests per rate, admission by free slots and "
+                   "recording memory, continuous batching into 256 slots, 10 ms bins per "
+                   "request; latency = wait (arrival to admission) + service" % count}
+
+
+def activity_sweep(conn, steps=SIM_STEPS, fracs=(0.001, 0.01, 0.10)):
+    """The plain single trial at 0.1 %, 1 % and 10 % Poisson drive (150 Hz)
+    for ``steps`` steps through ``fis.batch.Batch``: neuron-steps/s from CUDA
+    events around the device work, and spikes per step from the counts."""
+    import numpy as np
+    import torch
+
+    from fis.batch import Batch, TrialSpec
+
+    out = []
+    b = Batch(conn, 1, group=1)
+    for frac in fracs:
+        rng = np.random.default_rng(int(frac * 1e4) + 17)
+        stim = np.sort(rng.choice(conn.n, size=int(frac * conn.n), replace=False))
+        spec = TrialSpec(seed=1234 + int(frac * 1e4), steps=steps, stim=stim, rate_hz=150.0)
+        b.run([spec])  # warm
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        counts = b.run([spec])
+        e.record()
+        torch.cuda.synchronize()
+        ms = s.elapsed_time(e)
+        out.append({"drive_frac": frac, "driven": int(stim.size), "steps": steps,
+                    "value": conn.n * steps / (ms / 1000.0), "unit": "neuron-steps/s",
+                    "ms": ms, "spikes_per_step": float(counts.sum()) / steps})
+    del b
+    torch.cuda.empty_cache()
     return out
+
+
+def propagation_roofline(core, batch, specs, hbm, peak_kind, warm_blocks=10, blocks=20):
+    """Roofline of the propagation kernel (k_phase_a: the scatter of the spikes
+    that reach a block, and the block's Poisson drive), each launch timed alone
+    with CUDA events on its stream, over ``blocks`` blocks of the resident
+    64-trial workload at steady activity.
+
+    Algorithmic HBM bytes of one launch, from the spikes it delivers (those of
+    the previous block, read back from the trials' recordings): per spike
+    chunk (work item) its list entry (4 B) and row bounds (2 x 8 B), 4 B per
+    edge pushed, the rates of the group (4 B per trial-neuron) and the kick
+    words of driven neurons (4 B).  Each pushed edge is also one 32-bit atomic
+    add in L2, reported beside as L2 bytes (4 B read + 4 B written)."""
+    import numpy as np
+    import torch
+
+    dev = core.device
+    deg = torch.as_tensor(core.conn.out_degree().astype(np.int64), device=dev)
+    nch = core.nchunks.to(torch.int64)
+    rec = batch.last_recording[:, 0]          # [B][N] spikes so far, slot order
+    driven = (core.rates > 0).to(torch.int64)
+    for b in range(len(specs)):
+        t = core.trials[b]
+        t.start, t.end = core.step, core.step + (warm_blocks + blocks + 1) * core.max_block
+    core.mark_trials()
+    core.reset_slots(slice(None))
+    rec.zero_()
+    core.advance((warm_blocks - 1) * core.max_block)
+    prev = rec.clone()
+    core.advance(core.max_block)
+    G = core.group
+    evs, bytes_, edges = [], [], []
+    for _ in range(blocks):
+        pairs = []
+
+        def timer(st, start, pairs=pairs):
+            if start:
+                pairs.append([torch.cuda.Event(enable_timing=True),
+                              torch.cuda.Event(enable_timing=True)])
+            pairs[-1][0 if start else 1].record(torch.cuda.current_stream(dev))
+
+        cur = rec.clone()
+        delivered = cur - prev                # the spikes this block's scatter pushes
+        prev = cur
+        core.block(core.max_block, scatter_timer=timer)
+        for j, g0 in enumerate(range(0, core.batch, G)):
+            per = delivered[g0:g0 + G].sum(0)
+            items = int((per * nch).sum())
+            e = int((per * deg).sum())
+            nb = min(G, core.batch - g0)
+            b = 20 * items + 4 * e + 4 * nb * core.n + 4 * int(driven[g0:g0 + G].sum())
+            evs.append(pairs[j])
+            bytes_.append(b)
+            edges.append(e)
+    torch.cuda.synchronize()
+    ms = [a.elapsed_time(b) for a, b in evs]
+    core.check_errors()
+    sec = sum(ms) / 1000.0
+    achieved = sum(bytes_) / sec / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm, "traffic": None, "kernel": "k_phase_a",
+            "launch_ms": statistics.mean(ms), "launches": len(ms),
+            "algorithmic_bytes_per_launch": statistics.mean(bytes_),
+            "edges_per_launch": statistics.mean(edges),
+            "l2_atomic_gbs": 8.0 * sum(edges) / sec / 1e9, "peak_kind": peak_kind,
+            "how": "each phase-A launch alone (not overlapped), %d blocks of the 64-trial "
+                   "workload after %d warm blocks; bytes from the spikes each launch "
+                   "delivers" % (blocks, warm_blocks)}
 
 
 def dist_env():
@@ -396,21 +510,23 @@ def main():
         del eng
 
     hbm, peak_kind = peaks()
-    alg = None
     roof = None
     if upd_ms:
         G = core.group
-        bytes_launch = G * conn.n * UPDATE_BYTES_PER_NEURON_BLOCK
-        alg = bytes_launch
+        bytes_launch = G * conn.n * update_bytes_per_neuron_block(core)
         achieved = bytes_launch / (upd_ms / 1000.0) / 1e9
         roof = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm,
                 "traffic": NCU_TRAFFIC_PER_NEURON_BLOCK * G * conn.n,
                 "kernel": "k_update", "launch_ms": upd_ms,
-                "algorithmic_bytes_per_launch": alg, "peak_kind": peak_kind}
+                "algorithmic_bytes_per_launch": bytes_launch,
+                "bytes_per_neuron_block": update_bytes_per_neuron_block(core),
+                "peak_kind": peak_kind}
 
-    uneven = serving = None
-    if rank == 0 and not args.quick:
+    uneven = serving = sweep = prop = None
+    if rank == 0 and world == 1 and not args.quick:
+        prop = propagation_roofline(core, batch, specs, hbm, peak_kind)
+        sweep = activity_sweep(conn)
         uneven = uneven_run(conn, core.group)
         serving = serving_run(conn, core.group, plain["value"] if plain else None)
 
@@ -442,9 +558,11 @@ def main():
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": args.steps * blocks * core.launches_per_block(),
             "roofline": roof,
+            "roofline_propagation": prop,
             "plain_1trial": plain,
             "batched_over_plain": (value / world) / plain["value"] if plain else None,
             "uneven_256": uneven,
+            "activity_sweep_1trial": sweep,
             "serving": serving,
             "cpu_baseline": cpu,
         }

@@ -66,6 +66,16 @@ class Reply:
     def latency(self):
         return self.finished - self.arrival
 
+    @property
+    def wait(self):
+        """Time from arrival to admission (queued for slots or memory)."""
+        return self.admitted - self.arrival
+
+    @property
+    def service(self):
+        """Time from admission to the result on the host."""
+        return self.finished - self.admitted
+
 
 class Server:
     """Slots on one GPU, filled from a queue as they free up."""
@@ -218,11 +228,18 @@ class Server:
 
     @staticmethod
     def latency_stats(replies):
-        lat = np.array([r.latency for r in replies], dtype=np.float64)
-        if lat.size == 0:
+        """p50/p99/mean of the latency (arrival to result), and p50/p99 of its
+        two parts: the admission wait and the service time."""
+        if not replies:
             return {"p50_s": None, "p99_s": None, "n": 0}
-        return {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
-                "mean_s": float(lat.mean()), "n": int(lat.size)}
+        out = {"n": len(replies)}
+        for key, prefix in (("latency", ""), ("wait", "wait_"), ("service", "service_")):
+            x = np.array([getattr(r, key) for r in replies], dtype=np.float64)
+            out[prefix + "p50_s"] = float(np.percentile(x, 50))
+            out[prefix + "p99_s"] = float(np.percentile(x, 99))
+            if not prefix:
+                out["mean_s"] = float(x.mean())
+        return out
 
 
 def poisson_requests(n, seed, rate_hz, count, trials=(1, 64), steps=(1000, 50000),

@@ -6,7 +6,8 @@ to several hundred on this synthetic connectome (the 10 % run settles near
 40 Hz mean firing) and the scatter's load balance over the Pareto-tailed rows
 is exercised from nearly idle to busy.  Each run is compared with the oracle
 (the reference's step restated in C, pinned to the reference by
-test_oracle.py) bit for bit: per-neuron spike counts and the final state.
+test_oracle.py) bit for bit over the configuration's full 10,000 steps (1 s):
+per-neuron spike counts and the final state.
 """
 
 import numpy as np
@@ -16,7 +17,8 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-STEPS = 400
+STEPS = 10_000  # 1 s
+CHUNK = 1000    # oracle steps per call (bounds the raster it returns)
 
 
 @pytest.fixture(scope="module")
@@ -38,11 +40,18 @@ def test_activity_sweep_matches_oracle(conn, frac):
 
     o = O.Oracle.from_connectome(conn, batch=1, no_refractory=stim, seed=spec.seed, streams=[0])
     o.rates[0, stim] = np.float32(150.0)
-    raster = o.run(STEPS, raster=True)
-    bits = np.unpackbits(raster[:, 0], axis=1, bitorder="little")[:, :conn.n]
-    per_step = bits.sum(1)
+    want = np.zeros(conn.n, dtype=np.int64)
+    per_step = []
+    for _ in range(STEPS // CHUNK):
+        raster = o.run(CHUNK, raster=True)
+        bits = np.unpackbits(raster[:, 0], axis=1, bitorder="little")[:, :conn.n]
+        per_step.append(bits.sum(1))
+        want += bits.sum(0)
+    per_step = np.concatenate(per_step)
+    print("drive %.1f %%: %.1f spikes per step (max %d) over %d steps"
+          % (100 * frac, per_step.mean(), per_step.max(), STEPS))
     assert per_step.max() > 0
-    assert np.array_equal(counts, bits.sum(0))
+    assert np.array_equal(counts, want)
     core = b.core
     assert np.array_equal(core.v[0].cpu().numpy(), o.v[0])
     assert np.array_equal(core.g[0].cpu().numpy(), o.conductance[0])
