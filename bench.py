@@ -76,14 +76,17 @@ def parse():
     return ap.parse_args()
 
 
-def uneven_run(conn, group):
-    """256 trials, durations U[500, 20,000] steps, retired in place as they end."""
+def uneven_run(conn):
+    """256 trials, durations U[500, 20,000] steps, retired in place as they end,
+    with the launch shape tuned for a batch of 256 (widths 1-256)."""
     import torch
 
     from fis.batch import Batch, random_specs
+    from fis.tune import core_kwargs, tune
 
+    best = tune(conn, 256)
     specs = random_specs(conn.n, 256, SPEC_SEED + 7, (500, 20000))
-    b = Batch(conn, 256, group=group)
+    b = Batch(conn, 256, **core_kwargs(best))
     b.run(specs[:8])  # warm the allocations
     torch.cuda.synchronize()
     s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -97,14 +100,16 @@ def uneven_run(conn, group):
     torch.cuda.empty_cache()
     return {"value": trial_steps * conn.n / (ms / 1000.0), "unit": "neuron-steps/s",
             "trials": 256, "durations": "U[500, 20000] steps", "trial_steps": trial_steps,
-            "ms": ms, "how": "host trial specs in, host counts out; finished trials frozen "
-                             "in place until the longest ends"}
+            "ms": ms, "tuned": {k: best[k] for k in best if k != "candidates"},
+            "autotune_candidates": len(best["candidates"]),
+            "how": "host trial specs in, host counts out; finished trials frozen "
+                   "in place until the longest ends"}
 
 
 SERVING_RATES_HZ = (2.0, 10.0, 50.0)
 
 
-def serving_run(conn, group, plain_value, rates=SERVING_RATES_HZ, count=100):
+def serving_run(conn, launch, plain_value, rates=SERVING_RATES_HZ, count=100):
     """Open-loop streams of ``count`` requests at each Poisson arrival rate:
     1-64 trials and 1,000-50,000 steps per request, 10 ms bins.  Latency is
     arrival to result on the host; it splits into the admission wait (queued
@@ -114,7 +119,7 @@ def serving_run(conn, group, plain_value, rates=SERVING_RATES_HZ, count=100):
     from fis.serve import Server, poisson_requests
 
     lines = []
-    srv = Server(conn, capacity=256, group=group)
+    srv = Server(conn, capacity=256, **launch)
     for j, hz in enumerate(rates):
         reqs = poisson_requests(conn.n, SPEC_SEED + 9 + j, hz, count, trials=(1, 64),
                                 steps=(1000, 50000), bin_steps=100)
@@ -384,21 +389,19 @@ def main():
     import fis.connectome as C
     from fis.batch import Batch, random_specs
 
-    from fis.tune import tune
+    from fis.engine import Core
+    from fis.tune import core_kwargs, tune
 
     conn = C.synthetic(seed=CONN_SEED)
     specs = random_specs(conn.n, args.trials, SPEC_SEED + 1000 * rank, args.sim_steps)
     if args.group is None:
         best = tune(conn, args.trials)
     else:
-        best = {"group": args.group, "chunk": None, "candidates": []}
-    core = None
-    if args.block_steps is not None:
-        from fis.engine import Core
-
-        core = Core(conn, args.trials, group=best["group"], chunk=best["chunk"], raster=False,
-                    max_block=args.block_steps)
-    batch = Batch(conn, args.trials, group=best["group"], chunk=best["chunk"], core=core)
+        best = {"group": args.group, "chunk": None, "ring": None, "scatter_mode": None,
+                "scat_ctas": 0, "drive_ctas": 0, "candidates": []}
+    core = Core(conn, args.trials, raster=False, max_block=args.block_steps or 20,
+                **core_kwargs(best))
+    batch = Batch(conn, args.trials, core=core)
     core = batch.core
     slots = list(range(args.trials))
     batch.load(slots, specs)
@@ -527,8 +530,8 @@ def main():
     if rank == 0 and world == 1 and not args.quick:
         prop = propagation_roofline(core, batch, specs, hbm, peak_kind)
         sweep = activity_sweep(conn)
-        uneven = uneven_run(conn, core.group)
-        serving = serving_run(conn, core.group, plain["value"] if plain else None)
+        uneven = uneven_run(conn)
+        serving = serving_run(conn, core_kwargs(best), plain["value"] if plain else None)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -547,7 +550,11 @@ def main():
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "trials_per_gpu": args.trials,
-                       "sim_steps": args.sim_steps, "trial_group": core.group, "scatter_chunk": core.chunk,
+                       "sim_steps": args.sim_steps, "trial_group": core.group,
+                       "scatter_chunk": core.chunk,
+                       "ring": "int16 pairs" if core.ring16 else "int32",
+                       "scatter_mode": core.scatter_mode,
+                       "phase_a_ctas_per_8_sms": [core.scat_ctas, core.drive_ctas],
                        "autotune_candidates": len(best["candidates"]),
                        "block_steps": core.max_block,
                        "l2": "inputs larger than L2 (trial state 150 MB, spike lists "

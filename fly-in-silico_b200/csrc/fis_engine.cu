@@ -206,28 +206,16 @@ struct ScatterArgs {
 // The value that marks an empty pair of biased uint16 ring elements.
 constexpr uint32_t kEmptyPair = 0x80008000u;
 
-// The scatter's work for CTA `bid` of `nblk`; `pre_sum` holds (K+1)*nb+1 ints.
-__device__ __forceinline__ void scatter_body(const fis_engine& E, const ScatterArgs& A,
-                                             const int bid, const int nblk, int32_t* pre_sum) {
-  const int n = E.n;
+// Prefix sum of the lengths of the scatter's source lists into pre_sum
+// (entries [pre_sum[j], pre_sum[j+1]) of the concatenation are list j, j =
+// kk*nb + bl; list kk < nsrc holds step u_first + kk, the one after them the
+// list of step u_last); returns the total.  All threads of the CTA call it.
+__device__ __forceinline__ int32_t list_prefix(const fis_engine& E, const ScatterArgs& A,
+                                               const fis_clock& ck, int64_t u_first,
+                                               int64_t u_last, int slot2_last, int nlists,
+                                               int32_t* pre_sum) {
   const int B = E.batch;
   const int L = E.p.lag;
-  const fis_clock ck = A.clk_given ? A.clk : *E.clock;
-  const uint64_t keep = policy_keep();  // the ring stays in L2 for the update
-  const int64_t t0 = ck.step;
-  const int64_t u_first = t0 + A.u_off;  // u_off is -lag: u_first = t0 mod lag
-  const int64_t u_last = t0 - 1;
-  // slots of step u_first + kk: (ck.slot + kk) mod L and (ck.slot2 + L + kk) mod 2L
-  const int slot_last = wrap(ck.slot + L - 1, L);
-  const int slot2_last = wrap(ck.slot2 + 2 * L - 1, 2 * L);
-  const int t_mod_r = A.slot_mode ? (int)mod_pos(t0, E.p.buf_len) : 0;
-  // Is the list of step t0-1 one of the sources?
-  const int kk_last = (int)(u_last - u_first);
-  const bool last_is_src = A.filter_last && kk_last >= 0 && kk_last < A.nsrc;
-  const bool extra = A.filter_last && !last_is_src && u_last >= 0;
-  const int nlists = (A.nsrc + (extra ? 1 : 0)) * A.nb;
-
-  // Prefix sum of the list lengths: entries [j*..] of list j, j = kk*nb + bl.
   {
     const int per = (nlists + kScatThreads - 1) / kScatThreads;
     const int j0 = threadIdx.x * per;
@@ -268,7 +256,30 @@ __device__ __forceinline__ void scatter_body(const fis_engine& E, const ScatterA
     if (threadIdx.x == 0) pre_sum[nlists] = all;
     __syncthreads();
   }
-  const int32_t total = pre_sum[nlists];
+  return pre_sum[nlists];
+}
+
+// The scatter's work for CTA `bid` of `nblk`; `pre_sum` holds (K+1)*nb+1 ints.
+__device__ __forceinline__ void scatter_body(const fis_engine& E, const ScatterArgs& A,
+                                             const int bid, const int nblk, int32_t* pre_sum) {
+  const int n = E.n;
+  const int B = E.batch;
+  const int L = E.p.lag;
+  const fis_clock ck = A.clk_given ? A.clk : *E.clock;
+  const uint64_t keep = policy_keep();  // the ring stays in L2 for the update
+  const int64_t t0 = ck.step;
+  const int64_t u_first = t0 + A.u_off;  // u_off is -lag: u_first = t0 mod lag
+  const int64_t u_last = t0 - 1;
+  // slots of step u_first + kk: (ck.slot + kk) mod L and (ck.slot2 + L + kk) mod 2L
+  const int slot_last = wrap(ck.slot + L - 1, L);
+  const int slot2_last = wrap(ck.slot2 + 2 * L - 1, 2 * L);
+  const int t_mod_r = A.slot_mode ? (int)mod_pos(t0, E.p.buf_len) : 0;
+  // Is the list of step t0-1 one of the sources?
+  const int kk_last = (int)(u_last - u_first);
+  const bool last_is_src = A.filter_last && kk_last >= 0 && kk_last < A.nsrc;
+  const bool extra = A.filter_last && !last_is_src && u_last >= 0;
+  const int nlists = (A.nsrc + (extra ? 1 : 0)) * A.nb;
+  const int32_t total = list_prefix(E, A, ck, u_first, u_last, slot2_last, nlists, pre_sum);
 
   // Lists that the following update phase will write start empty.
   if (bid == 0) {
@@ -362,6 +373,9 @@ __device__ __forceinline__ void scatter_body(const fis_engine& E, const ScatterA
 constexpr int kDriveThreads = 256;
 constexpr int kDriveSpan = 256;  // neurons per warp task
 
+// kAllLoads: read the span's eight rate words before the first ballot (one
+// round trip per task) instead of four at a time.
+template <bool kAllLoads>
 __device__ __forceinline__ void drive_body(const fis_engine& E, const int b0, const int nb,
                                            const int K, const fis_clock& clk,
                                            const int clk_given, const int bid, const int nblk) {
@@ -388,10 +402,19 @@ __device__ __forceinline__ void drive_body(const fis_engine& E, const int b0, co
     if (ka >= kb) continue;  // uniform across the warp
     const float* rates = E.rates + (int64_t)b * n;
     int cnt = 0;
-#pragma unroll 4
+    float pr[kDriveSpan / kWarp];
+    if (kAllLoads) {
+#pragma unroll
+      for (int c = 0; c < kDriveSpan / kWarp; ++c) {
+        const int i = i0 + c * kWarp + lane;
+        pr[c] = i < n ? ld_hint(rates + i, stream) : 0.f;
+      }
+    }
+#pragma unroll(kAllLoads ? kDriveSpan / kWarp : 4)
     for (int c = 0; c < kDriveSpan / kWarp; ++c) {
       const int i = i0 + c * kWarp + lane;
-      const float p = i < n ? __fmul_rn(ld_hint(rates + i, stream), E.p.prob_scale) : 0.f;
+      const float rate = kAllLoads ? pr[c] : (i < n ? ld_hint(rates + i, stream) : 0.f);
+      const float p = i < n ? __fmul_rn(rate, E.p.prob_scale) : 0.f;
       const bool d = p > 0.f;
       const unsigned m = __ballot_sync(0xFFFFFFFFu, d);
       if (d) {
@@ -431,11 +454,161 @@ __device__ __forceinline__ void drive_body(const fis_engine& E, const int b0, co
   }
 }
 
+// ---------------------------------------------------------------------------
+// phase A, balanced form (scatter_mode 1): a warp per 32 work items
+// ---------------------------------------------------------------------------
+//
+// The same work as scatter_body -- the same lists, filtering and atomics --
+// with the memory round trips of 32 work items taken together.  Each lane
+// resolves one item (its list by binary search over pre_sum, its entry, its
+// row bounds: three round trips for all 32), and the warp then walks the
+// concatenation of the items' edges as 16-byte quads, 32 quads per pass and
+// kScatUnroll passes' loads in flight per lane before their atomics.  A lane
+// finds the item of its quad by a binary search over the lanes' exclusive
+// prefix sums of quad counts.  Item ranges start anywhere in the edge array;
+// a quad is read from its 16-byte aligned address and only the edges inside
+// the item's range are pushed.
+constexpr int kScatUnroll = 4;
+
+__device__ __forceinline__ void scatter_body_warp(const fis_engine& E, const ScatterArgs& A,
+                                                  const int bid, const int nblk,
+                                                  int32_t* pre_sum) {
+  const int n = E.n;
+  const int B = E.batch;
+  const int L = E.p.lag;
+  const fis_clock ck = A.clk_given ? A.clk : *E.clock;
+  const uint64_t keep = policy_keep();
+  const int64_t t0 = ck.step;
+  const int64_t u_first = t0 + A.u_off;
+  const int64_t u_last = t0 - 1;
+  const int slot_last = wrap(ck.slot + L - 1, L);
+  const int slot2_last = wrap(ck.slot2 + 2 * L - 1, 2 * L);
+  const int t_mod_r = A.slot_mode ? (int)mod_pos(t0, E.p.buf_len) : 0;
+  const int kk_last = (int)(u_last - u_first);
+  const bool last_is_src = A.filter_last && kk_last >= 0 && kk_last < A.nsrc;
+  const bool extra = A.filter_last && !last_is_src && u_last >= 0;
+  const int nlists = (A.nsrc + (extra ? 1 : 0)) * A.nb;
+  const int32_t total = list_prefix(E, A, ck, u_first, u_last, slot2_last, nlists, pre_sum);
+  if (bid == 0) {
+    for (int j = threadIdx.x; j < A.zero_next * A.nb; j += blockDim.x) {
+      const int kk = j / A.nb, bl = j - kk * A.nb;
+      E.list_len[wrap(ck.slot2 + kk, 2 * L) * B + A.b0 + bl] = 0;
+    }
+  }
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int warp = threadIdx.x / kWarp;
+  const int rows_per_slot = A.half ? (A.nb + 1) >> 1 : A.nb;
+  constexpr unsigned kAll = 0xFFFFFFFFu;
+  for (int32_t w0 = (bid * kScatWarps + warp) * kWarp; w0 < total;
+       w0 += nblk * kScatWarps * kWarp) {
+    // this lane's work item: quads [q0, q0 + nq) of edges, of which edges
+    // [q0*4 + lo, q0*4 + hi) are the item's, pushed into ring row `row`
+    const int32_t w = w0 + lane;
+    int64_t q0 = 0;
+    int nq = 0;
+    uint32_t span = 0;  // lo | hi << 2 (lo < 4, hi <= chunk + 3)
+    uint32_t row = 0;   // ring row | (upper half of a paired word) << 31
+    if (w < total) {
+      int lo = 0, hi = nlists - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pre_sum[mid] <= w) lo = mid; else hi = mid - 1;
+      }
+      const int j = lo;
+      const int kk = j / A.nb, bl = j - kk * A.nb;
+      const int b = A.b0 + bl;
+      const bool is_src = kk < A.nsrc;
+      const int64_t u = is_src ? u_first + kk : u_last;
+      const int su = is_src ? wrap(ck.slot + kk, L) : slot_last;
+      uint32_t* lst = E.lists + ((int64_t)su * B + b) * E.list_cap;
+      const int32_t idx = w - pre_sum[j];
+      uint32_t e = kDeadEntry;
+      if (idx < E.list_cap) e = lst[idx];
+      const uint32_t pre = entry_pre(e);
+      bool live = e != kDeadEntry && pre < (uint32_t)n;
+      if (live && A.filter_last && u == u_last) {
+        const uint8_t fl = E.flags[(int64_t)b * n + pre];
+        if (fl & (FIS_FL_OUT_OFF | FIS_FL_SILENCED)) {
+          if (!is_src) lst[idx] = kDeadEntry;
+          live = false;
+        }
+      }
+      if (live && is_src) {
+        const int64_t r0 = E.row_ptr[pre], r1 = E.row_ptr[pre + 1];
+        const int64_t lo_e = r0 + (int64_t)entry_chunk(e) * E.chunk;
+        const int64_t hi_e = min(r1, lo_e + (int64_t)E.chunk);
+        if (lo_e < hi_e) {
+          q0 = lo_e >> 2;
+          nq = (int)(((hi_e + 3) >> 2) - q0);
+          span = (uint32_t)(lo_e - q0 * 4) | ((uint32_t)(hi_e - q0 * 4) << 2);
+          const int slot = A.slot_mode ? wrap(t_mod_r + kk, E.p.buf_len) : kk;
+          row = (uint32_t)(slot * rows_per_slot + (A.half ? bl >> 1 : bl)) |
+                ((uint32_t)(A.half && (bl & 1)) << 31);
+        }
+      }
+    }
+    if (!__any_sync(kAll, nq > 0)) continue;
+    int inc = nq;
+#pragma unroll
+    for (int off = 1; off < kWarp; off <<= 1) {
+      const int t = __shfl_up_sync(kAll, inc, off);
+      if (lane >= off) inc += t;
+    }
+    const int all = __shfl_sync(kAll, inc, kWarp - 1);
+    const int ex = inc - nq;
+    for (int j0 = 0; j0 < all; j0 += kWarp * kScatUnroll) {
+      uint4 q[kScatUnroll];
+      int lo[kScatUnroll], hi[kScatUnroll];
+      uint32_t rw[kScatUnroll];
+#pragma unroll
+      for (int v = 0; v < kScatUnroll; ++v) {
+        const int j = j0 + kWarp * v + lane;
+        int r = 0;
+#pragma unroll
+        for (int step = kWarp / 2; step > 0; step >>= 1) {
+          const int c = r + step;
+          if (__shfl_sync(kAll, ex, c) <= j) r = c;
+        }
+        const int qi = j - __shfl_sync(kAll, ex, r);
+        const int64_t qa = __shfl_sync(kAll, q0, r) + qi;
+        const uint32_t sp = __shfl_sync(kAll, span, r);
+        rw[v] = __shfl_sync(kAll, row, r);
+        lo[v] = (int)(sp & 3u) - 4 * qi;
+        hi[v] = j < all ? (int)(sp >> 2) - 4 * qi : 0;  // hi <= 0: nothing to push
+        if (hi[v] > 0) q[v] = __ldg(reinterpret_cast<const uint4*>(E.edges) + qa);
+      }
+#pragma unroll
+      for (int v = 0; v < kScatUnroll; ++v) {
+        if (hi[v] <= 0) continue;
+        const uint32_t wv[4] = {q[v].x, q[v].y, q[v].z, q[v].w};
+        const int64_t base = (int64_t)(rw[v] & 0x7FFFFFFFu) * A.trial_stride;
+        const int shift = (rw[v] >> 31) ? 16 : 0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          if (c >= lo[v] && c < hi[v]) {
+            const int post = edge_post(wv[c]);
+            if (post < n) {
+              if (A.half)
+                red_hint(reinterpret_cast<uint32_t*>(A.ring + base) + post,
+                         (uint32_t)edge_count(wv[c]) << shift, keep);
+              else
+                red_hint(A.ring + base + post, edge_count(wv[c]), keep);
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
 // The scatter alone (the delay-ring readout uses it).
 __global__ void __launch_bounds__(kScatThreads)
 k_scatter(const fis_engine E, const ScatterArgs A) {
   extern __shared__ int32_t pre_sum[];
-  scatter_body(E, A, blockIdx.x, gridDim.x, pre_sum);
+  if (E.scatter_mode == 1)
+    scatter_body_warp(E, A, blockIdx.x, gridDim.x, pre_sum);
+  else
+    scatter_body(E, A, blockIdx.x, gridDim.x, pre_sum);
 }
 
 // Phase A of a block as one grid: CTAs [0, scat) scatter, the rest draw the
@@ -444,15 +617,23 @@ k_scatter(const fis_engine E, const ScatterArgs A) {
 // runs beside the previous group's update, whose CTAs fill the register
 // file: at 32 registers a thread (a few bytes of the Philox draw spill to L1)
 // two phase-A CTAs take the room of one update CTA instead of 1.5.
+// The balanced scatter (kMode 1) keeps four passes of quads in flight and is
+// held to 48 registers a thread instead (five CTAs in the room of four
+// update CTAs); it needs fewer CTAs for the same work.
 static_assert(kScatThreads == kDriveThreads, "one block size for both roles");
-__global__ void __launch_bounds__(kScatThreads, 7)
+template <int kMode>
+__global__ void __launch_bounds__(kScatThreads, kMode ? 5 : 7)
 k_phase_a(const fis_engine E, const ScatterArgs A, const int scat) {
   extern __shared__ int32_t pre_sum[];
-  if ((int)blockIdx.x < scat)
-    scatter_body(E, A, blockIdx.x, scat, pre_sum);
-  else
-    drive_body(E, A.b0, A.nb, A.nsrc, A.clk, A.clk_given, blockIdx.x - scat,
-               gridDim.x - scat);
+  if ((int)blockIdx.x < scat) {
+    if (kMode == 1)
+      scatter_body_warp(E, A, blockIdx.x, scat, pre_sum);
+    else
+      scatter_body(E, A, blockIdx.x, scat, pre_sum);
+  } else {
+    drive_body<kMode == 1>(E, A.b0, A.nb, A.nsrc, A.clk, A.clk_given, blockIdx.x - scat,
+                           gridDim.x - scat);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1137,6 +1318,9 @@ int fis_check(const fis_engine* e) {
   if (e->list_cap < 1) return FIS_E_ARG;
   if (e->p.lag < 2 || e->p.buf_len != e->p.lag - 1) return FIS_E_ARG;
   if (e->n_recs < 0 || (e->n_recs > 0 && !e->recs)) return FIS_E_ARG;
+  if (e->scatter_mode < 0 || e->scatter_mode > 1) return FIS_E_ARG;
+  if (e->scat_ctas < 0 || e->drive_ctas < 0 || e->scat_ctas > 256 || e->drive_ctas > 256)
+    return FIS_E_ARG;
   if (!aligned16(e->edges)) return FIS_E_ALIGN;
   return FIS_OK;
 }
@@ -1207,16 +1391,26 @@ int scatter_block(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, 
   // smallest that still ends within an update.  Up to 1.5 scattering and 3
   // drawing CTAs per SM (4.5 per SM, one wave at 5 per SM) measured best on
   // the full connectome for trial groups of 16 to 64.
+  // The balanced scatter (mode 1), which keeps more loads in flight per
+  // warp, defaults to one scattering and two drawing CTAs per SM.  The
+  // descriptor may set both counts (per 8 SMs, for the autotuner).
+  const bool balanced = e->scatter_mode == 1;
   int drive = 0;
   if (!e->vstim && k_steps > 1) {
     const int64_t warps = (int64_t)nb * ((e->n + kDriveSpan - 1) / kDriveSpan);
-    const int64_t cap = (int64_t)sm_count() * 3;
+    const int64_t cap = e->drive_ctas > 0 ? std::max(1, sm_count() * e->drive_ctas / 8)
+                                          : (int64_t)sm_count() * (balanced ? 2 : 3);
     const int64_t blocks = (warps + kDriveThreads / kWarp - 1) / (kDriveThreads / kWarp);
     drive = (int)(blocks < cap ? blocks : cap);
   }
-  const int scat = drive ? std::max(sm_count(), sm_count() * std::min(per_sm, 3) / 2)
-                         : sm_count() * per_sm;
-  k_phase_a<<<scat + drive, kScatThreads, smem, st>>>(*e, A, scat);
+  int scat = drive ? std::max(sm_count(), sm_count() * std::min(per_sm, 3) / 2)
+                   : sm_count() * per_sm;
+  if (balanced && drive) scat = sm_count();
+  if (e->scat_ctas > 0) scat = std::max(1, sm_count() * e->scat_ctas / 8);
+  if (balanced)
+    k_phase_a<1><<<scat + drive, kScatThreads, smem, st>>>(*e, A, scat);
+  else
+    k_phase_a<0><<<scat + drive, kScatThreads, smem, st>>>(*e, A, scat);
   return launch_status();
 }
 

@@ -126,10 +126,12 @@ class Batch:
     """
 
     def __init__(self, conn: Connectome, capacity: int, params=None, device="cuda",
-                 group=None, chunk=None, core: Core | None = None):
-        # results come from recordings: no per-step raster needed
+                 group=None, chunk=None, core: Core | None = None, **launch):
+        # results come from recordings: no per-step raster needed.  `launch`:
+        # the remaining Core arguments of a tuning result (ring,
+        # scatter_mode, scat_ctas, drive_ctas)
         self.core = core or Core(conn, capacity, params=params, device=device, group=group,
-                                 chunk=chunk, raster=False)
+                                 chunk=chunk, raster=False, **launch)
         self.n = self.core.n
         self.capacity = self.core.batch
         self._copy_stream = None  # the side stream of the counts' copy to the host

@@ -82,9 +82,9 @@ class Server:
 
     def __init__(self, conn: Connectome, capacity: int = 256, params=None, device="cuda",
                  group=None, chunk=None, memory_budget: int | None = None,
-                 advance_steps: int = 200):
+                 advance_steps: int = 200, **launch):
         self.batch = Batch(conn, capacity, params=params, device=device, group=group,
-                           chunk=chunk)
+                           chunk=chunk, **launch)
         self.core = self.batch.core
         self.n = self.core.n
         self.capacity = capacity

@@ -1,21 +1,30 @@
 """Autotuner for the block launch shape, cached per (N, E, batch, GPU).
 
-Tunables (all exact: they change scheduling, never results):
+Tunables (all exact: they change scheduling and storage, never results):
 
-* ``group`` -- trials per launch of the block (the batch width of one
-  scatter + update pair).  Narrow groups keep the scratch ring
-  ([K][group][NR] int32) resident in L2; wide groups cut launches and the
+* ``group`` -- the batch width of one launch pair (trials per phase-A +
+  update launch), from 1 up to the whole batch (8-256 at a batch of 256).
+  Narrow groups keep the scratch ring in L2; wide groups cut launches and the
   tail of the last wave.
-* ``chunk`` -- edges per scatter work item (a warp walks one chunk of one
-  spiking row): the load balance over the Pareto-tailed out-degrees.
+* ``ring`` -- the scratch ring's layout: ``int16`` interleaves two trials in
+  each 32-bit word (rows of trial pairs, half the bytes; exact when no
+  neuron's incoming |count| sum reaches 2**15), ``int32`` one row per trial.
+* ``scatter_mode`` -- the warps a spiking row gets: 0 = a warp per work item
+  (spike, chunk of its row), i.e. ceil(degree / chunk) warps per row, one
+  item per warp at a time; 1 = 32 work items per warp, resolved together and
+  walked as one stream of edge quads (a row shares its warp with up to 31
+  others).
+* ``chunk`` -- edges per work item (the row split behind warps-per-row):
+  256, 512 or 1024.
+* ``scat_ctas`` / ``drive_ctas`` -- phase-A CTAs per 8 SMs for the scatter and
+  the Poisson drive (0 = the library's default for the mode).
 
-The ring layout is fixed (trial-major rows padded to 256 neurons, one update
-CTA per trial tile); the block length is the delay lag (20 steps), the longest
-that keeps steps within a block independent.
-
-Each candidate runs a short seeded trial mix on a scratch engine and is timed
-with CUDA events; the winner is stored in a JSON cache (``FIS_TUNE_CACHE`` or
-``~/.cache/fis/tune.json``).
+The block length stays the delay lag (20 steps), the longest that keeps the
+steps of a block independent.  The search is coordinate-wise: group x ring at
+the default launch, then scatter mode x chunk at the best of those, then the
+phase-A grid.  Each candidate runs a short seeded trial mix on a scratch
+engine and is timed with CUDA events; the winner is stored in a JSON cache
+(``FIS_TUNE_CACHE`` or ``~/.cache/fis/tune.json``).
 """
 
 from __future__ import annotations
@@ -30,6 +39,8 @@ import torch
 from .connectome import Connectome
 from .engine import Core
 
+KEYS = ("group", "ring", "scatter_mode", "chunk", "scat_ctas", "drive_ctas")
+
 
 def cache_path() -> Path:
     p = os.environ.get("FIS_TUNE_CACHE")
@@ -38,7 +49,7 @@ def cache_path() -> Path:
 
 def _key(conn: Connectome, batch: int) -> str:
     name = torch.cuda.get_device_name() if torch.cuda.is_available() else "cpu"
-    return "%s|n=%d|e=%d|b=%d" % (name, conn.n, conn.nnz, batch)
+    return "%s|n=%d|e=%d|b=%d|v2" % (name, conn.n, conn.nnz, batch)
 
 
 def load_cache() -> dict:
@@ -79,39 +90,90 @@ def _time(core: Core, steps: int, reps: int) -> float:
     return best / steps
 
 
-def tune(conn: Connectome, batch: int, params=None, groups=None, chunks=None, steps=400,
-         reps=2, use_cache=True, verbose=False) -> dict:
-    """Best ``{"group", "chunk", "ms_per_step"}`` for this connectome and batch."""
+def default_groups(batch):
+    return sorted({g for g in (1, 2, 4, 8, 16, 32, 64, 128, 256) if g <= batch} | {batch})
+
+
+def tune(conn: Connectome, batch: int, params=None, groups=None, rings=None, modes=(1, 0),
+         chunks=None, grids=None, steps=400, reps=2, use_cache=True, verbose=False) -> dict:
+    """Best launch shape ``{group, ring, scatter_mode, chunk, scat_ctas,
+    drive_ctas, ms_per_step, candidates}`` for this connectome and batch."""
     key = _key(conn, batch)
     cache = load_cache() if use_cache else {}
     if key in cache:
         return cache[key]
-    deg = conn.out_degree()
-    maxdeg = int(deg.max()) if conn.n else 0
+    maxdeg = int(conn.out_degree().max()) if conn.n else 0
     base_chunk = max(256, 128 * -(-maxdeg // (255 * 128)))
     chunks = chunks or sorted({base_chunk, max(base_chunk, 512), max(base_chunk, 1024)})
-    groups = groups or sorted({g for g in (1, 2, 4, 8, 16, 32, 64, 128, 256) if g <= batch}
-                              | {batch})
+    groups = groups or default_groups(batch)
+    fits16 = conn.exactness()["max_abs_row_sum"] < (1 << 15)
+    rings = rings or (["int16", "int32"] if fits16 else ["int32"])
+    grids = grids or [(8, 16), (8, 8), (4, 16), (12, 16), (8, 24), (16, 24)]
     results = []
-    for chunk in chunks:
-        core = Core(conn, batch, params=params, chunk=chunk, group=groups[0], raster=False)
-        _mix(core)
+    cores = {}
+
+    def core_for(ring, chunk):
+        if (ring, chunk) not in cores:
+            cores.clear()
+            torch.cuda.empty_cache()
+            c = Core(conn, batch, params=params, chunk=chunk, group=groups[0], ring=ring,
+                     raster=False)
+            _mix(c)
+            cores[(ring, chunk)] = c
+        return cores[(ring, chunk)]
+
+    def seen(cand):
+        return any(all(r[k] == cand[k] for k in KEYS) for r in results)
+
+    def trial(cand):
+        c = core_for(cand["ring"], cand["chunk"])
+        c.set_group(cand["group"])
+        c.set_launch(cand["scatter_mode"], cand["scat_ctas"], cand["drive_ctas"])
+        ms = _time(c, steps, reps)
+        results.append(dict(cand, ms_per_step=ms))
+        if verbose:
+            print("tune: %s  %.4f ms/step" % (" ".join("%s=%s" % (k, cand[k]) for k in KEYS), ms),
+                  flush=True)
+
+    def best_so_far():
+        return {k: min(results, key=lambda r: r["ms_per_step"])[k] for k in KEYS}
+
+    best = {"group": groups[0], "ring": rings[0], "scatter_mode": modes[0],
+            "chunk": base_chunk, "scat_ctas": 0, "drive_ctas": 0}
+    # 1. batch width x ring layout at the default launch
+    for ring in rings:
         for g in groups:
-            core.set_group(g)
-            ms = _time(core, steps, reps)
-            results.append({"group": g, "chunk": chunk, "ms_per_step": ms})
-            if verbose:
-                print("tune: group %3d chunk %4d  %.4f ms/step" % (g, chunk, ms), flush=True)
-        del core
-        torch.cuda.empty_cache()
-    best = min(results, key=lambda r: r["ms_per_step"])
-    best = dict(best, candidates=results)
+            trial(dict(best, ring=ring, group=g))
+    best = best_so_far()
+    # 2. warps per row: scatter mode x chunk
+    for chunk in chunks:
+        for mode in modes:
+            cand = dict(best, chunk=chunk, scatter_mode=mode)
+            if not seen(cand):
+                trial(cand)
+    best = best_so_far()
+    # 3. the phase-A grid for that mode
+    for sc, dr in grids:
+        cand = dict(best, scat_ctas=sc, drive_ctas=dr)
+        if not seen(cand):
+            trial(cand)
+    cores.clear()
+    torch.cuda.empty_cache()
+    win = min(results, key=lambda r: r["ms_per_step"])
+    out = dict(win, candidates=results)
     if use_cache:
-        cache[key] = best
+        cache[key] = out
         try:
             p = cache_path()
             p.parent.mkdir(parents=True, exist_ok=True)
             p.write_text(json.dumps(cache, indent=1))
         except OSError:
             pass
-    return best
+    return out
+
+
+def core_kwargs(best: dict) -> dict:
+    """The Core arguments of a tuning result."""
+    return {"group": best["group"], "chunk": best.get("chunk"), "ring": best.get("ring"),
+            "scatter_mode": best.get("scatter_mode"), "scat_ctas": best.get("scat_ctas", 0),
+            "drive_ctas": best.get("drive_ctas", 0)}

@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define FIS_ABI_VERSION 6
+#define FIS_ABI_VERSION 7
 
 /* Largest number of steps one block may advance (registers per thread). */
 #define FIS_MAX_BLOCK 20
@@ -162,6 +162,16 @@ typedef struct fis_engine {
                          0: only of each block's last step (all the next
                          block needs), for runs that read spikes through
                          recordings and spike lists alone                  */
+  int32_t scatter_mode;  /* how the scatter spreads its work items (spike,
+                            chunk of a row) over warps: 0 = one item per warp
+                            at a time; 1 = 32 items per warp, resolved
+                            together, their edges walked as one stream of
+                            16-byte quads.  Same sums either way.          */
+  int32_t scat_ctas;     /* phase-A CTAs that scatter, per 8 SMs (0 = the
+                            library's default for the mode)                 */
+  int32_t drive_ctas;    /* phase-A CTAs that draw the Poisson drive, per 8
+                            SMs (0 = default)                                */
+  int32_t pad2_;
   fis_lif_params p;
 } fis_engine;
 

@@ -28,7 +28,7 @@ def raster_rows(core, first, last):
     return out
 
 
-def make_engine(name, graphs=False, group=None, ring=None):
+def make_engine(name, graphs=False, group=None, ring=None, scatter_mode=None):
     from fis import sim
 
     sc = S.SCENARIOS[name]
@@ -36,6 +36,8 @@ def make_engine(name, graphs=False, group=None, ring=None):
     eng = sim.build_engine(weights=conn, silenced=S.silenced(sc), params=sc["params"],
                            batch=sc["batch"], seed=sc["seed"], no_refractory=S.driven(sc),
                            graphs=graphs, group=group, ring=ring)
+    if scatter_mode is not None:
+        eng.core.set_launch(scatter_mode)
     return sc, eng
 
 
@@ -95,10 +97,12 @@ def test_tape_driven_core_matches_reference(name, golden):
 @pytest.mark.parametrize("name", SMALL)
 @pytest.mark.parametrize("group", [None, 1, 2])
 @pytest.mark.parametrize("ring", ["int16", "int32"])
-def test_blocked_stepping_matches_reference(name, group, ring, golden):
-    """Blocks of up to 20 fused steps, split only where the masks change."""
+@pytest.mark.parametrize("scatter_mode", [0, 1])
+def test_blocked_stepping_matches_reference(name, group, ring, scatter_mode, golden):
+    """Blocks of up to 20 fused steps, split only where the masks change; both
+    scatter forms (a warp per work item, a warp per 32 items)."""
     z = golden(name)
-    sc, eng = make_engine(name, group=group, ring=ring)
+    sc, eng = make_engine(name, group=group, ring=ring, scatter_mode=scatter_mode)
     assert eng.core.ring16 == (ring == "int16")
     core = eng.core
     core.rates.copy_(torch.from_numpy(S.rates_matrix(sc)))
@@ -120,10 +124,11 @@ def test_blocked_stepping_matches_reference(name, group, ring, golden):
     assert final_state_equal(eng, z) == []
 
 
-def test_full_size_config0_matches_reference(golden):
+@pytest.mark.parametrize("scatter_mode", [0, 1])
+def test_full_size_config0_matches_reference(scatter_mode, golden):
     """138,639 neurons, 15.09 M edges, 1,000 steps in 20-step blocks."""
     z = golden("full_cfg0")
-    sc, eng = make_engine("full_cfg0")
+    sc, eng = make_engine("full_cfg0", scatter_mode=scatter_mode)
     core = eng.core
     core.rates.copy_(torch.from_numpy(S.rates_matrix(sc)))
     rows = []
