@@ -556,6 +556,10 @@ def main():
                        "scatter_mode": core.scatter_mode,
                        "phase_a_ctas_per_8_sms": [core.scat_ctas, core.drive_ctas],
                        "autotune_candidates": len(best["candidates"]),
+                       "autotune": [[c[k] for k in ("group", "ring", "scatter_mode", "chunk",
+                                                    "scat_ctas", "drive_ctas")]
+                                    + [round(c["ms_per_step"] * 1000.0, 2)]
+                                    for c in best["candidates"]],
                        "block_steps": core.max_block,
                        "l2": "inputs larger than L2 (trial state 150 MB, spike lists "
                              "%.0f MB, CSR 60 MB)" % (core.lists.numel() * 4 / 1e6),

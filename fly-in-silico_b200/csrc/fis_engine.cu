@@ -455,13 +455,13 @@ __device__ __forceinline__ void drive_body(const fis_engine& E, const int b0, co
 }
 
 // ---------------------------------------------------------------------------
-// phase A, balanced form (scatter_mode 1): a warp per 32 work items
+// phase A, balanced form (scatter_mode 1): a warp per task of up to 32 items
 // ---------------------------------------------------------------------------
 //
 // The same work as scatter_body -- the same lists, filtering and atomics --
-// with the memory round trips of 32 work items taken together.  Each lane
-// resolves one item (its list by binary search over pre_sum, its entry, its
-// row bounds: three round trips for all 32), and the warp then walks the
+// with the memory round trips of a task of work items taken together.  Each
+// lane resolves one item (its list by binary search over pre_sum, its entry,
+// its row bounds: three round trips for the whole task), and the warp walks the
 // concatenation of the items' edges as 16-byte quads, 32 quads per pass and
 // kScatUnroll passes' loads in flight per lane before their atomics.  A lane
 // finds the item of its quad by a binary search over the lanes' exclusive
@@ -499,16 +499,21 @@ __device__ __forceinline__ void scatter_body_warp(const fis_engine& E, const Sca
   const int warp = threadIdx.x / kWarp;
   const int rows_per_slot = A.half ? (A.nb + 1) >> 1 : A.nb;
   constexpr unsigned kAll = 0xFFFFFFFFu;
-  for (int32_t w0 = (bid * kScatWarps + warp) * kWarp; w0 < total;
-       w0 += nblk * kScatWarps * kWarp) {
+  // Items per warp task: about two tasks per warp of the grid, 1 to 32.  A
+  // light load (one step of one trial) spreads over many warps as one item
+  // each; a heavy one packs 32 items into each task.
+  const int tw = nblk * kScatWarps;
+  const int per = max(1, min(kWarp, total / (2 * tw)));
+  const int32_t tasks = (total + per - 1) / per;
+  for (int32_t task = bid * kScatWarps + warp; task < tasks; task += tw) {
     // this lane's work item: quads [q0, q0 + nq) of edges, of which edges
     // [q0*4 + lo, q0*4 + hi) are the item's, pushed into ring row `row`
-    const int32_t w = w0 + lane;
+    const int32_t w = task * per + lane;
     int64_t q0 = 0;
     int nq = 0;
     uint32_t span = 0;  // lo | hi << 2 (lo < 4, hi <= chunk + 3)
     uint32_t row = 0;   // ring row | (upper half of a paired word) << 31
-    if (w < total) {
+    if (lane < per && w < total) {
       int lo = 0, hi = nlists - 1;
       while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
@@ -973,7 +978,7 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
     drv_any = drv_any || (valid && runs[t] && __fmul_rn(rate[t], E.p.prob_scale) > 0.f);
     bitrow[t] = E.bits + ((int64_t)(b0 + 2 * pp + (t < nt ? t : 0)) * Wd + (i >> 5)) * L;
     s_prev[t] = false;
-    if (runs[t] && warp_valid && t0 - 1 >= tr[t].start && t0 >= 1)
+    if (runs[t] && warp_valid && t0 - 1 >= tr[t].start - tr[t].history && t0 >= 1)
       s_prev[t] = (bitrow[t][slot0 == 0 ? L - 1 : slot0 - 1] >> lane) & 1u;
   }
   const bool warp_driven = !kTape && __any_sync(0xFFFFFFFFu, drv_any);

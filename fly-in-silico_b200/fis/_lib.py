@@ -64,7 +64,7 @@ class Trial(ctypes.Structure):
                 ("end", ctypes.c_int64), ("v_clamp", ctypes.c_float),
                 ("stream", ctypes.c_uint32), ("rec", ctypes.c_int32),
                 ("bin_steps", ctypes.c_int32), ("n_bins", ctypes.c_int32),
-                ("pad_", ctypes.c_int32)]
+                ("history", ctypes.c_int32)]
 
 
 class EngineDesc(ctypes.Structure):

@@ -238,6 +238,7 @@ class Batch:
             t.stream = 0
             t.start = start
             t.end = start + int(s.steps)
+            t.history = 0
             t.v_clamp = float(np.float32(c.pdict["vReset"] if s.v_clamp is None else s.v_clamp))
             if shared is not None:
                 ri, nb = shared, int(rec.shape[0])

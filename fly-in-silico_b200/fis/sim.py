@@ -722,6 +722,9 @@ class Engine:
                 c.trials[b].seed = int(rec["seed"][b])
                 c.trials[b].stream = int(rec["stream"][b])
             c.trials[b].start = t - int(own[b])
+            # the spikes of step t-1 loaded below are this trial's, also when
+            # its own step restarts at t (generator state dropped)
+            c.trials[b].history = 1
         c.mark_trials()
         c._sync_trials()
         if self.graded:

@@ -11,9 +11,9 @@ Tunables (all exact: they change scheduling and storage, never results):
   neuron's incoming |count| sum reaches 2**15), ``int32`` one row per trial.
 * ``scatter_mode`` -- the warps a spiking row gets: 0 = a warp per work item
   (spike, chunk of its row), i.e. ceil(degree / chunk) warps per row, one
-  item per warp at a time; 1 = 32 work items per warp, resolved together and
-  walked as one stream of edge quads (a row shares its warp with up to 31
-  others).
+  item per warp at a time; 1 = tasks of 1-32 work items per warp (about two
+  tasks per warp of the grid), resolved together and walked as one stream of
+  edge quads (a row shares its warp with up to 31 others).
 * ``chunk`` -- edges per work item (the row split behind warps-per-row):
   256, 512 or 1024.
 * ``scat_ctas`` / ``drive_ctas`` -- phase-A CTAs per 8 SMs for the scatter and
@@ -49,7 +49,7 @@ def cache_path() -> Path:
 
 def _key(conn: Connectome, batch: int) -> str:
     name = torch.cuda.get_device_name() if torch.cuda.is_available() else "cpu"
-    return "%s|n=%d|e=%d|b=%d|v2" % (name, conn.n, conn.nnz, batch)
+    return "%s|n=%d|e=%d|b=%d|v3" % (name, conn.n, conn.nnz, batch)
 
 
 def load_cache() -> dict:
@@ -95,7 +95,7 @@ def default_groups(batch):
 
 
 def tune(conn: Connectome, batch: int, params=None, groups=None, rings=None, modes=(1, 0),
-         chunks=None, grids=None, steps=400, reps=2, use_cache=True, verbose=False) -> dict:
+         chunks=None, grids=None, steps=1000, reps=2, use_cache=True, verbose=False) -> dict:
     """Best launch shape ``{group, ring, scatter_mode, chunk, scat_ctas,
     drive_ctas, ms_per_step, candidates}`` for this connectome and batch."""
     key = _key(conn, batch)

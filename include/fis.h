@@ -100,7 +100,10 @@ typedef struct fis_trial {
   int32_t rec;        /* recording buffer index, -1 = no recording           */
   int32_t bin_steps;  /* own steps per recording bin                         */
   int32_t n_bins;     /* bins in the recording buffer                        */
-  int32_t pad_;
+  int32_t history;    /* steps before `start` whose spikes are the trial's
+                         own (1 after a restore that loaded the spikes of
+                         step start-1; 0 for a fresh trial, whose slot may
+                         hold a previous occupant's raster)                 */
 } fis_trial;
 
 /*

@@ -46,7 +46,7 @@ def test_activity_sweep_matches_oracle(conn, frac):
         raster = o.run(CHUNK, raster=True)
         bits = np.unpackbits(raster[:, 0], axis=1, bitorder="little")[:, :conn.n]
         per_step.append(bits.sum(1))
-        want += bits.sum(0)
+        want += bits.sum(0).astype(np.int64)
     per_step = np.concatenate(per_step)
     print("drive %.1f %%: %.1f spikes per step (max %d) over %d steps"
           % (100 * frac, per_step.mean(), per_step.max(), STEPS))

@@ -86,7 +86,8 @@ def test_uneven_mix_against_float64_on_sampled_trials():
         while left > 0:                  # 200 ms pieces bound the raster's size
             k = min(left, 2000)
             r = o.run_f64(k, raster=True)
-            total += np.unpackbits(r[:, 0], axis=1, bitorder="little")[:, :conn.n].sum(0)
+            total += np.unpackbits(r[:, 0], axis=1,
+                                   bitorder="little")[:, :conn.n].sum(0).astype(np.int64)
             left -= k
         seconds = s.steps * 1e-4         # 0.1 ms steps
         m = compare_rates(whole[j] / seconds, total / seconds)
