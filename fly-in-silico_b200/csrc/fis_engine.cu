@@ -35,6 +35,7 @@
 
 #include <algorithm>
 #include <mutex>
+#include <vector>
 
 #include "fis_common.cuh"
 
@@ -1326,6 +1327,7 @@ int fis_check(const fis_engine* e) {
   if (e->scatter_mode < 0 || e->scatter_mode > 1) return FIS_E_ARG;
   if (e->scat_ctas < 0 || e->drive_ctas < 0 || e->scat_ctas > 256 || e->drive_ctas > 256)
     return FIS_E_ARG;
+  if (e->update_streams < 0 || e->update_streams > 2) return FIS_E_ARG;
   if (!aligned16(e->edges)) return FIS_E_ALIGN;
   return FIS_OK;
 }
@@ -1464,9 +1466,11 @@ int check_advance(const fis_engine* e, int64_t start, int64_t steps, int32_t gro
 // use and kept for the life of the process.
 struct OverlapRes {
   cudaStream_t side = nullptr;
+  cudaStream_t upd2 = nullptr;                    // second update stream
   cudaEvent_t after_sc[2] = {nullptr, nullptr};   // scatter of launch l done (l mod 2)
-  cudaEvent_t after_upd[2] = {nullptr, nullptr};  // update of launch l done (l mod 2)
+  std::vector<cudaEvent_t> after_upd;             // update of launch l done (l mod size)
   cudaEvent_t start = nullptr;                    // the call's starting point
+  cudaEvent_t upd2_done = nullptr;                // the second update stream's last work
 };
 constexpr int kMaxOverlapDevices = 64;
 std::mutex g_overlap_mu;  // held for a whole call: the events are shared
@@ -1489,12 +1493,23 @@ int overlap_res(OverlapRes** out) {
     for (int j = 0; j < 2; ++j) {
       if ((err = cudaEventCreateWithFlags(&r.after_sc[j], cudaEventDisableTiming)))
         return (int)err;
-      if ((err = cudaEventCreateWithFlags(&r.after_upd[j], cudaEventDisableTiming)))
-        return (int)err;
     }
+    if ((err = cudaStreamCreateWithFlags(&r.upd2, cudaStreamNonBlocking))) return (int)err;
+    if ((err = cudaEventCreateWithFlags(&r.upd2_done, cudaEventDisableTiming))) return (int)err;
     if ((err = cudaEventCreateWithFlags(&r.start, cudaEventDisableTiming))) return (int)err;
   }
   *out = &r;
+  return FIS_OK;
+}
+
+// At least `n` update events in R (created on first need, kept for the process).
+int overlap_events(OverlapRes* R, size_t n) {
+  while (R->after_upd.size() < n) {
+    cudaEvent_t ev = nullptr;
+    const cudaError_t err = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (err != cudaSuccess) return (int)err;
+    R->after_upd.push_back(ev);
+  }
   return FIS_OK;
 }
 
@@ -1562,14 +1577,24 @@ int fis_advance_overlap(const fis_engine* e, int64_t start, int64_t steps, int32
   std::lock_guard<std::mutex> lk(g_overlap_mu);
   OverlapRes* R = nullptr;
   if ((rc = overlap_res(&R))) return rc;
+  // Launch l (over all blocks and groups, in order) uses ring l mod 2.  Its
+  // scatter runs on the side stream and waits for update l - 2, which
+  // drained that ring, and for update l - ngroups, the same trial group one
+  // block earlier, which wrote the spike lists the scatter reads; its update
+  // waits for that scatter and for update l - ngroups (the group's state).
+  // So each update overlaps the scatter of the next launch, across block
+  // boundaries too.  With two update streams (e->update_streams == 2 and at
+  // least two trial groups), consecutive updates -- of different groups,
+  // hence independent -- alternate between the caller's stream and a second
+  // one, so the tail of one update grid overlaps the start of the next.
+  const int64_t ngroups = (B + group - 1) / group;
+  const int nstreams = (e->update_streams == 2 && ngroups >= 2) ? 2 : 1;
+  const int64_t M = ngroups + 2;  // update events kept: launches l-M .. l-1
+  if ((rc = overlap_events(R, (size_t)M))) return rc;
   cudaStream_t st = (cudaStream_t)stream;
-  // Scatters run on the side stream, updates on the caller's stream, launch
-  // l (over all blocks and groups, in order) using ring l mod 2.  Scatter l
-  // waits only for update l - 2, which drained its ring and -- updates
-  // running in order -- also wrote every spike list the scatter reads (those
-  // of the same trial group one block earlier); so each update overlaps the
-  // scatter of the next launch, across block boundaries too.
+  cudaStream_t ust[2] = {st, R->upd2};
   if ((rc = (int)cudaEventRecord(R->start, st))) return rc;
+  if (nstreams == 2 && (rc = (int)cudaStreamWaitEvent(R->upd2, R->start, 0))) return rc;
   int64_t done = 0;
   int64_t launch = 0;
   while (done < steps) {
@@ -1581,19 +1606,33 @@ int fis_advance_overlap(const fis_engine* e, int64_t start, int64_t steps, int32
       const int32_t nb = (B - g0) < group ? (B - g0) : group;
       const bool last = final_block && g0 + nb == B;  // advances the device clock
       const int r = (int)(launch & 1);
-      cudaEvent_t dep = launch >= 2 ? R->after_upd[r] : R->start;
-      if ((rc = (int)cudaStreamWaitEvent(R->side, dep, 0))) return rc;
+      cudaStream_t us = ust[nstreams == 2 ? r : 0];
+      if (launch >= 2) {
+        if ((rc = (int)cudaStreamWaitEvent(R->side, R->after_upd[(launch - 2) % M], 0)))
+          return rc;
+      } else if ((rc = (int)cudaStreamWaitEvent(R->side, R->start, 0))) {
+        return rc;
+      }
+      cudaEvent_t same_group = launch >= ngroups ? R->after_upd[(launch - ngroups) % M]
+                                                 : nullptr;
+      if (same_group && (rc = (int)cudaStreamWaitEvent(R->side, same_group, 0))) return rc;
       if ((rc = scatter_block(e, g0, nb, k, rings[r], R->side, &clk))) return rc;
       if ((rc = (int)cudaEventRecord(R->after_sc[r], R->side))) return rc;
-      if ((rc = (int)cudaStreamWaitEvent(st, R->after_sc[r], 0))) return rc;
+      if ((rc = (int)cudaStreamWaitEvent(us, R->after_sc[r], 0))) return rc;
+      if (same_group && nstreams == 2 && (rc = (int)cudaStreamWaitEvent(us, same_group, 0)))
+        return rc;
       const bool timed = events && (launch % every) == 0 && (launch / every) < n_pairs;
-      if ((rc = record_if(timed, events, 2 * (launch / every), st))) return rc;
-      if ((rc = update_block(e, g0, nb, k, rings[r], sp, last, st, &clk))) return rc;
-      if ((rc = record_if(timed, events, 2 * (launch / every) + 1, st))) return rc;
-      if ((rc = (int)cudaEventRecord(R->after_upd[r], st))) return rc;
+      if ((rc = record_if(timed, events, 2 * (launch / every), us))) return rc;
+      if ((rc = update_block(e, g0, nb, k, rings[r], sp, last, us, &clk))) return rc;
+      if ((rc = record_if(timed, events, 2 * (launch / every) + 1, us))) return rc;
+      if ((rc = (int)cudaEventRecord(R->after_upd[launch % M], us))) return rc;
       ++launch;
     }
     done += k;
+  }
+  if (nstreams == 2) {  // later work on the caller's stream follows both
+    if ((rc = (int)cudaEventRecord(R->upd2_done, R->upd2))) return rc;
+    if ((rc = (int)cudaStreamWaitEvent(st, R->upd2_done, 0))) return rc;
   }
   return FIS_OK;
 }

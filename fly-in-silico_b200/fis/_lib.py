@@ -83,7 +83,7 @@ class EngineDesc(ctypes.Structure):
                 ("wait_polls", ctypes.c_uint32), ("inject_stall", ctypes.c_uint32),
                 ("raster", ctypes.c_int32), ("scatter_mode", ctypes.c_int32),
                 ("scat_ctas", ctypes.c_int32), ("drive_ctas", ctypes.c_int32),
-                ("pad2_", ctypes.c_int32), ("p", LifParams)]
+                ("update_streams", ctypes.c_int32), ("p", LifParams)]
 
 
 _lib = None

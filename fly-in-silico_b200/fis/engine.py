@@ -87,7 +87,8 @@ class Core:
 
     def __init__(self, conn: Connectome, batch: int, params=None, device="cuda",
                  group=None, chunk=None, max_block=_lib.FIS_MAX_BLOCK, ring=None,
-                 overlap=True, raster=True, scatter_mode=None, scat_ctas=0, drive_ctas=0):
+                 overlap=True, raster=True, scatter_mode=None, scat_ctas=0, drive_ctas=0,
+                 update_streams=1):
         self.device = require_cuda(device)
         self.lib = _lib.load()
         conn.check_bounds()
@@ -198,25 +199,29 @@ class Core:
         d.ring16 = 1 if self.ring16 else 0
         d.raster = 1 if self.raster else 0
         d.p = self.P
-        self.set_launch(scatter_mode, scat_ctas, drive_ctas)
+        self.set_launch(scatter_mode, scat_ctas, drive_ctas, update_streams)
 
-    def set_launch(self, scatter_mode=None, scat_ctas=0, drive_ctas=0):
+    def set_launch(self, scatter_mode=None, scat_ctas=0, drive_ctas=0, update_streams=1):
         """Phase A's launch shape (exact: it changes scheduling, never sums).
 
         ``scatter_mode`` 0: a warp walks one work item (spike, row chunk) at a
         time; 1: a warp resolves 32 items together and walks their edges as
         one stream (None: ``FIS_SCATTER_MODE``, else 1).  ``scat_ctas`` and
         ``drive_ctas``: scattering and drive CTAs per 8 SMs (0: the library's
-        default for the mode).
+        default for the mode).  ``update_streams`` 2: in the overlapped native
+        loop, consecutive updates (of different trial groups) alternate
+        between two streams.
         """
         if scatter_mode is None:
             scatter_mode = int(os.environ.get("FIS_SCATTER_MODE", "1"))
         d = self.desc
         d.scatter_mode, d.scat_ctas, d.drive_ctas = (int(scatter_mode), int(scat_ctas),
                                                      int(drive_ctas))
+        d.update_streams = int(update_streams)
         _lib.check(self.lib.fis_check(ctypes.byref(d)), "fis_check")
         self.scatter_mode, self.scat_ctas, self.drive_ctas = (int(scatter_mode), int(scat_ctas),
                                                                int(drive_ctas))
+        self.update_streams = int(update_streams)
 
     def check_errors(self):
         """Raise if a kernel flagged an error since the last check (synchronises).

@@ -174,7 +174,9 @@ typedef struct fis_engine {
                             library's default for the mode)                 */
   int32_t drive_ctas;    /* phase-A CTAs that draw the Poisson drive, per 8
                             SMs (0 = default)                                */
-  int32_t pad2_;
+  int32_t update_streams;  /* fis_advance_overlap: 2 = consecutive updates
+                              (of different trial groups) alternate between
+                              the caller's stream and a second one; else 1 */
   fis_lif_params p;
 } fis_engine;
 
@@ -273,8 +275,10 @@ int fis_advance(const fis_engine* e, int64_t start, int64_t steps, int32_t group
  * library-owned side stream, one per device) runs while the previous update
  * runs on `stream`, across block boundaries too: launch l (over all blocks
  * and groups, in order) uses ring l mod 2 and its scatter waits only for
- * update l - 2.  On return all work is ordered before later work on
- * `stream`.
+ * update l - 2 and for the previous block's update of the same trial group.
+ * With e->update_streams == 2 and two or more trial groups, consecutive
+ * updates alternate between `stream` and a second library-owned stream.
+ * On return all work is ordered before later work on `stream`.
  *   ring2  two consecutive rings of fis_block's layout, each for
  *          min(FIS_MAX_BLOCK, lag) slots and min(group, rows or batch)
  *          trials, empty on entry and on return

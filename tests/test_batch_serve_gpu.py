@@ -110,8 +110,11 @@ def test_server_latency_stats_and_budget():
 
 @pytest.mark.parametrize("ring", ["int16", "int32"])
 @pytest.mark.parametrize("scatter_mode", [0, 1])
-def test_overlapped_advance_equals_sequential(ring, scatter_mode):
-    """Scatter/update overlap on two rings gives the one-ring result, bit for bit."""
+@pytest.mark.parametrize("update_streams,group", [(1, 2), (2, 2), (2, 3)])
+def test_overlapped_advance_equals_sequential(ring, scatter_mode, update_streams, group):
+    """Scatter/update overlap on two rings (updates on one or two streams,
+    an even and an odd number of trial groups) gives the one-ring result, bit
+    for bit."""
     from fis.batch import Batch
     from fis.engine import Core
 
@@ -119,7 +122,8 @@ def test_overlapped_advance_equals_sequential(ring, scatter_mode):
     sp = specs(61, 7, (150, 300))   # uneven: trial groups drop out as they end
     got = []
     for overlap in (False, True):
-        core = Core(c, 7, group=2, ring=ring, overlap=overlap, scatter_mode=scatter_mode)
+        core = Core(c, 7, group=group, ring=ring, overlap=overlap, scatter_mode=scatter_mode,
+                    update_streams=update_streams)
         counts = Batch(c, 7, core=core).run(sp)
         got.append((counts, core.v.cpu().numpy(), core.g.cpu().numpy(),
                     core.refrac.cpu().numpy(), core.step))
