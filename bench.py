@@ -171,6 +171,35 @@ def activity_sweep(conn, steps=SIM_STEPS, fracs=(0.001, 0.01, 0.10)):
     return out
 
 
+def red_rate_peak(device, words=16 << 20, iters=256):
+    """The sustained rate of 32-bit L2 atomic adds (adds per second), from the
+    library's calibration kernel on a 64 MB buffer that stays in L2: the
+    ceiling of the scatter, which makes one such add per pushed synapse."""
+    import ctypes
+
+    import torch
+
+    import fis._lib as L
+
+    lib = L.load()
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    ctas = sms * 8
+    buf = torch.zeros(words, dtype=torch.int32, device=device)
+    st = ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+    best = 0.0
+    for rep in range(4):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        L.check(lib.fis_red_rate(ctypes.c_void_p(buf.data_ptr()), words, iters, ctas, st),
+                "fis_red_rate")
+        e.record()
+        torch.cuda.synchronize(device)
+        if rep:  # the first launch warms the buffer into L2
+            best = max(best, ctas * 256 * iters / (s.elapsed_time(e) / 1000.0))
+    del buf
+    return best
+
+
 def propagation_roofline(core, batch, specs, hbm, peak_kind, warm_blocks=10, blocks=20):
     """Roofline of the propagation kernel (k_phase_a: the scatter of the spikes
     that reach a block, and the block's Poisson drive), each launch timed alone
@@ -229,15 +258,21 @@ def propagation_roofline(core, batch, specs, hbm, peak_kind, warm_blocks=10, blo
     core.check_errors()
     sec = sum(ms) / 1000.0
     achieved = sum(bytes_) / sec / 1e9
-    return {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-            "frac": achieved / hbm, "traffic": None, "kernel": "k_phase_a",
+    adds = sum(edges) / sec
+    red_peak = red_rate_peak(dev)
+    return {"bound": "l2_atomics", "achieved": adds / 1e9, "peak": red_peak / 1e9,
+            "unit": "G atomic adds/s", "frac": adds / red_peak,
+            "peak_kind": "measured here: fis_red_rate, random 32-bit red.add into 64 MB in L2",
+            "hbm": {"achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                    "peak_kind": peak_kind},
+            "traffic": None, "kernel": "k_phase_a",
             "launch_ms": statistics.mean(ms), "launches": len(ms),
             "algorithmic_bytes_per_launch": statistics.mean(bytes_),
             "edges_per_launch": statistics.mean(edges),
-            "l2_atomic_gbs": 8.0 * sum(edges) / sec / 1e9, "peak_kind": peak_kind,
+            "l2_atomic_gbs": 8.0 * adds / 1e9,
             "how": "each phase-A launch alone (not overlapped), %d blocks of the 64-trial "
-                   "workload after %d warm blocks; bytes from the spikes each launch "
-                   "delivers" % (blocks, warm_blocks)}
+                   "workload after %d warm blocks; bytes and atomic adds from the spikes "
+                   "each launch delivers" % (blocks, warm_blocks)}
 
 
 def dist_env():

@@ -102,8 +102,10 @@ __device__ __forceinline__ void bulk_store(void* gmem, const void* smem, unsigne
 __device__ __forceinline__ void bulk_commit() {
   asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
 }
+// Wait until the committed bulk copies have read their shared-memory source
+// (the CTA may then end; the global writes complete before the grid does).
 __device__ __forceinline__ void bulk_wait_all() {
-  asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
+  asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
 }
 // Order this thread's generic-proxy shared-memory writes before later
 // async-proxy (bulk copy) reads of them.
@@ -1169,8 +1171,9 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
   }
   }  // a trial of the pair runs in this block
 
-  // The clearing copies complete before the CTA ends (szero must stay valid
-  // while they read it, and the next scatter adds into these lines).
+  // The clearing copies have read szero before the CTA ends (it must stay
+  // valid while they read it); their writes into the ring are complete when
+  // the grid is, before the next scatter, a later kernel, adds into them.
   if (threadIdx.x < kWarp) bulk_wait_all();
   }  // the staged input arrived
 

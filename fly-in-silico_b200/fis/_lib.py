@@ -43,7 +43,7 @@ EXPORTS = ("ev_spmv_i32", "ev_spmv_i64", "ev_spmv_abi", "fis_abi",
            "fis_scatter", "fis_update", "fis_advance", "fis_advance_overlap",
            "fis_delay_buffer", "fis_spikes_f32", "fis_load_spikes", "fis_add_rows",
            "fis_graded_step",
-           "fis_ring_row", "fis_block_noalloc")
+           "fis_ring_row", "fis_block_noalloc", "fis_red_rate")
 
 
 class KernelUnavailable(RuntimeError):
@@ -116,6 +116,7 @@ def load(path=None):
     L.fis_advance.argtypes = [P, I64, I64, I32, I32, P, P, P, I32, I32, P]
     L.fis_advance_overlap.argtypes = [P, I64, I64, I32, I32, P, P, P, I32, I32, P]
     L.fis_update.argtypes = [P, I32, I32, I32, P, P, I32, P]
+    L.fis_red_rate.argtypes = [P, I64, I32, I32, P]
     L.fis_delay_buffer.argtypes = [P, I32, I32, P, P, P]
     L.fis_spikes_f32.argtypes = [P, I32, I32, I64, P, P]
     L.fis_load_spikes.argtypes = [P, I32, I32, P, P]

@@ -21,7 +21,7 @@ CSRC = ROOT / "csrc"
 INCLUDE = ROOT.parent / "include"
 OUT = PKG / "libfis_b200.so"
 
-SOURCES = ("fis_engine.cu", "fis_evspmv.cu", "fis_graded.cu")
+SOURCES = ("fis_engine.cu", "fis_evspmv.cu", "fis_graded.cu", "fis_calibrate.cu")
 ARCH = "-gencode=arch=compute_100a,code=sm_100a"
 
 

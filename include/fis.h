@@ -351,6 +351,15 @@ int fis_graded_step(const fis_engine* e, int64_t step, const int64_t* t_ptr,
 int fis_ring_row(int32_t n);
 
 /*
+ * Measurement aid, no counterpart in the reference: `ctas` CTAs of 256
+ * threads each add 1 (red.add.u32) at `iters` pseudo-random words of
+ * buf[0, words) -- ctas * 256 * iters atomic adds in all.  Timed by the
+ * caller, it gives the sustained L2 atomic-add rate that bounds the scatter
+ * (one such add per pushed synapse).  iters: a positive multiple of 8.
+ */
+int fis_red_rate(uint32_t* buf, int64_t words, int32_t iters, int32_t ctas, void* stream);
+
+/*
  * fis_block without the `ring` argument: the scratch ring is a fixed array
  * of FIS_NOALLOC_RING_INTS int32 (12 MiB) inside this library, for callers
  * that cannot allocate device memory (a real-time closed-loop controller,
