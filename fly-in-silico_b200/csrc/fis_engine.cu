@@ -943,14 +943,8 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
       if (!kTape && K > 1) dm[t] = ld_hint(E.kicks + sidx[t], stream);
     }
   }
-  // this neuron's chunk count, for the spike lists of the epilogue
-  const int nch = valid ? (int)E.nchunks[i] : 0;
   __syncthreads();  // the staging barrier exists before anyone waits on it
   const int64_t t0 = ck.step;
-  int32_t* recp[2];  // the trials' recording buffers, read long before the epilogue
-#pragma unroll
-  for (int t = 0; t < 2; ++t)
-    recp[t] = (tr[t].rec >= 0 && tr[t].rec < E.n_recs) ? E.recs[tr[t].rec] : nullptr;
   const int slot0 = ck.slot;  // ring-of-lists slot of step t0
   int ka[2], kb[2];
   bool runs[2];
@@ -1127,28 +1121,36 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
   up2(st.r, orr[0], orr[1]);
   up2(st.keep, okeep[0], okeep[1]);
   up2(nspk, ospk[0], ospk[1]);
+  // Addresses and trial fields are derived again here rather than kept live
+  // through the step loop (its register budget); the spike path reloads
+  // what it needs from L1.
 #pragma unroll
   for (int t = 0; t < 2; ++t) {
     if (!runs[t]) continue;
     const int b = b0 + 2 * pp + t;
+    const int64_t si = (int64_t)b * n + i;
     // the raster words of the K steps into the ring of the last L steps
     if (!only_last && lane < K && warp_valid) {
       const int sl = slot0 + lane < L ? slot0 + lane : slot0 + lane - L;
-      bitrow[t][sl] = sbal[t][wib][lane];
+      E.bits[((int64_t)b * Wd + (i >> 5)) * L + sl] = sbal[t][wib][lane];
     }
     if (valid) {
-      st_hint(E.v + sidx[t], ov[t], stream);
-      st_hint(E.g + sidx[t], og[t], stream);
-      st_hint(E.refrac + sidx[t], orr[t], stream);
-      if (spikes_out) spikes_out[sidx[t]] = (okeep[t] == 0.f) ? 1.f : 0.f;
+      st_hint(E.v + si, ov[t], stream);
+      st_hint(E.g + si, og[t], stream);
+      st_hint(E.refrac + si, orr[t], stream);
+      if (spikes_out) spikes_out[si] = (okeep[t] == 0.f) ? 1.f : 0.f;
     }
     // Spike lists and recording for the (rare) steps this neuron fired.
     uint32_t fired = (uint32_t)ospk[t];  // bit j is step K-1-j
     if (fired) {
       const int B = E.batch;
-      const bool out_on = !(fl[t] & (FIS_FL_OUT_OFF | FIS_FL_SILENCED));
+      const fis_trial trl = E.trials[b];
+      const uint32_t flb = E.flags[si];
+      const int nch = (int)E.nchunks[i];
+      int32_t* const recb = (trl.rec >= 0 && trl.rec < E.n_recs) ? E.recs[trl.rec] : nullptr;
+      const bool out_on = !(flb & (FIS_FL_OUT_OFF | FIS_FL_SILENCED));
       const int slot20 = ck.slot2;
-      const int64_t own0 = t0 - tr[t].start;
+      const int64_t own0 = t0 - trl.start;
       while (fired) {
         const int k = K - __ffs(fired);
         fired &= fired - 1;
@@ -1160,11 +1162,11 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
           for (int q = 0; q < nch; ++q)
             if (pos + q < E.list_cap) dst[pos + q] = ((uint32_t)i << 8) | (uint32_t)q;
         }
-        if (tr[t].rec >= 0 && tr[t].rec < E.n_recs && tr[t].bin_steps > 0) {
+        if (recb && trl.bin_steps > 0) {
           const int64_t own = own0 + k;
-          const int64_t bin = own < 0x7FFFFFFF ? (int64_t)((int)own / tr[t].bin_steps)
-                                                : own / tr[t].bin_steps;
-          if (bin < tr[t].n_bins) red_hint(recp[t] + bin * n + i, 1, stream);
+          const int64_t bin = own < 0x7FFFFFFF ? (int64_t)((int)own / trl.bin_steps)
+                                                : own / trl.bin_steps;
+          if (bin < trl.n_bins) red_hint(recb + bin * n + i, 1, stream);
         }
       }
     }
