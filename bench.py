@@ -40,11 +40,11 @@ WORKLOAD = ("batched 64 trials x 10,000 steps (1 s), N=138,639, E=15,091,983 syn
 SPEC_SEED = 2024
 CONN_SEED = 0
 # Update-kernel DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum)
-# per trial-neuron and block, from one ncu capture of a 16-trial, 20-step
-# launch at steady activity (187.0 MB; ncu flushes caches between replay
-# passes, so the scratch ring counts as cold reads and its clearing as DRAM
-# writes).  Scaled to the bench's launch size by the neurons it processes.
-NCU_TRAFFIC_PER_NEURON_BLOCK = 187.04e6 / (16 * 138_639)
+# per trial-neuron and block, from one ncu capture of an 8-trial, 20-step
+# launch at steady activity with the caches kept warm, as the live pipeline
+# leaves them (85.2 MB: the scratch ring is partly served from L2).  Scaled to
+# the bench's launch size by the neurons it processes.
+NCU_TRAFFIC_PER_NEURON_BLOCK = 85.20e6 / (8 * 138_639)
 
 
 def update_bytes_per_neuron_block(core):
