@@ -433,7 +433,8 @@ def main():
         best = tune(conn, args.trials)
     else:
         best = {"group": args.group, "chunk": None, "ring": None, "scatter_mode": None,
-                "scat_ctas": 0, "drive_ctas": 0, "update_streams": 1, "candidates": []}
+                "scat_ctas": 0, "drive_ctas": 0, "update_streams": 1, "update_tiles": None,
+                "candidates": []}
     core = Core(conn, args.trials, raster=False, max_block=args.block_steps or 20,
                 **core_kwargs(best))
     batch = Batch(conn, args.trials, core=core)
@@ -592,9 +593,10 @@ def main():
                        "phase_a_ctas_per_8_sms": [core.scat_ctas, core.drive_ctas],
                        "autotune_candidates": len(best["candidates"]),
                        "update_streams": core.update_streams,
+                       "update_tiles": core.update_tiles,
                        "autotune": [[c[k] for k in ("group", "ring", "scatter_mode", "chunk",
                                                     "scat_ctas", "drive_ctas",
-                                                    "update_streams")]
+                                                    "update_streams", "update_tiles")]
                                     + [round(c["ms_per_step"] * 1000.0, 2)]
                                     for c in best["candidates"]],
                        "block_steps": core.max_block,

@@ -865,25 +865,72 @@ __device__ __forceinline__ f2 step_loop2(Pair& st, const Consts& C, const fis_en
 // Everything the CTA reads is requested at entry -- the staged input (bulk
 // copies), the clock and trial records, the neuron state -- so their
 // latencies overlap each other and the drive computation.
+// Warp 0 of a CTA: stage the K slots of `tile` for trial pair `pp` into
+// `srow` with bulk copies (TMA) completing on `bar`, which it sets up.
+template <bool kHalf>
+__device__ __forceinline__ void stage_tile(const fis_engine& E, const int32_t* ring,
+                                           const int nb, const int K, const int pp,
+                                           const int tile,
+                                           int32_t (*srow)[StagedRow<kHalf>::kWords],
+                                           uint64_t* bar) {
+  const int NR = ring_row(E.n);
+  const int nt = (2 * pp + 1 < nb) ? 2 : 1;
+  const int np = (nb + 1) >> 1;
+  const int64_t sstride = kHalf ? (int64_t)np * NR * 2 : (int64_t)nb * NR;
+  const int64_t toff = kHalf ? ((int64_t)pp * NR + tile * kTile) * 2
+                             : (int64_t)(2 * pp) * NR + tile * kTile;
+  const int copies = kHalf ? K : K * nt;
+  const uint64_t keep = policy_keep();
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+    mbar_arrive_expect_tx(bar, (unsigned)copies * kTile * 4u);
+  }
+  __syncwarp();
+  if (!E.inject_stall) {
+    for (int c = threadIdx.x; c < copies; c += kWarp) {
+      const int k = kHalf ? c : c / nt, t = kHalf ? 0 : c - k * nt;
+      const int64_t off = (int64_t)k * sstride + toff + (int64_t)t * NR;
+      const void* src = kHalf ? (const void*)(reinterpret_cast<const uint16_t*>(ring) + off)
+                              : (const void*)(ring + off);
+      bulk_load(&srow[k][t * kTile], src, kTile * 4u, bar, keep);
+    }
+  }
+}
+
+// Four-byte async copy global -> shared (sm_80+), and the wait for all of this
+// thread's outstanding ones.
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem, uint64_t pol) {
+  asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], 4, %2;\n" ::"r"(
+                   smem_addr(smem)),
+               "l"(gmem), "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+// One tile's update: everything but the issue of its staging copies (warp 0
+// of the CTA has issued them into `srow`, completing on `bar`) and the clock
+// bump.  `pre`: this tile's v, g, refrac, rates and kicks ([5][2][threads]),
+// prefetched into shared memory by this thread's async copies, or null to read
+// them here.  `count`: this CTA counts itself in for the clock bump (into
+// *arrived) after the staging barrier.
 template <bool kTape, bool kHalf>
-__global__ void __launch_bounds__(kUpdThreads, 4)
-k_update(const fis_engine E, const int b0, const int nb, const int K,
-         int32_t* __restrict__ ring, float* __restrict__ spikes_out,
-         const int bump, const float unit,  // unit: 1.0f (see addp)
-         const fis_clock clk, const int clk_given) {
-  // The block's delayed input, a column per thread (per trial for int32):
-  // staged so the step loop stays rolled (a compact body that fits the
-  // instruction cache) and can index it by step.
-  __shared__ __align__(128) int32_t sring[FIS_MAX_BLOCK][StagedRow<kHalf>::kWords];
-  __shared__ __align__(16) uint32_t szero[kTile];                  // source of the clearing
-  __shared__ uint32_t sbal[2][kUpdThreads / kWarp][FIS_MAX_BLOCK]; // raster words per step
-  __shared__ __align__(8) uint64_t sbar;                           // staging barrier
+__device__ __forceinline__ void update_tile(
+    const fis_engine& E, const int b0, const int nb, const int K, int32_t* __restrict__ ring,
+    float* __restrict__ spikes_out, const float unit, const fis_clock& ck, const int tile,
+    int32_t (*srow)[StagedRow<kHalf>::kWords], uint64_t* bar, uint32_t* szero,
+    uint32_t (*sbal)[kUpdThreads / kWarp][FIS_MAX_BLOCK], const float* pre, const bool count,
+    unsigned* arrived) {
   const int n = E.n;
   const int L = E.p.lag;
   const int Wd = (n + kWarp - 1) / kWarp;
   const int NR = ring_row(n);
   const int pp = blockIdx.y;    // pair of trials of the group: 2 pp, 2 pp + 1
-  const int tile = blockIdx.x;  // 256-neuron tile
   const int i = tile * kTile + threadIdx.x;
   const int lane = threadIdx.x & (kWarp - 1);
   const int wib = threadIdx.x / kWarp;
@@ -899,30 +946,11 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
   const uint64_t keep = policy_keep();      // the scratch ring
   const uint64_t stream = policy_stream();  // the trial state
 
-  // Stage the tile's K slots: warp 0 sets up the barrier and issues the bulk
-  // copies (TMA), all completing on that barrier.
-  if (threadIdx.x < kWarp) {
-    if (threadIdx.x == 0) {
-      mbar_init(&sbar, 1);
-      fence_mbar_init();
-      mbar_arrive_expect_tx(&sbar, (unsigned)copies * kTile * 4u);
-    }
-    __syncwarp();
-    if (!E.inject_stall) {
-      for (int c = threadIdx.x; c < copies; c += kWarp) {
-        const int k = kHalf ? c : c / nt, t = kHalf ? 0 : c - k * nt;
-        const int64_t off = (int64_t)k * sstride + toff + (int64_t)t * NR;
-        const void* src = kHalf ? (const void*)(reinterpret_cast<const uint16_t*>(ring) + off)
-                                : (const void*)(ring + off);
-        bulk_load(&sring[k][t * kTile], src, kTile * 4u, &sbar, keep);
-      }
-    }
-  }
+  __syncwarp();  // sbal of the previous tile is read before this one writes it
 
   // Clock, trial records and state, requested before anything depends on
   // them.  A trial slot that does not run in this block is inert: its state
   // is not used, its threshold infinite, nothing of it stored.
-  const fis_clock ck = clk_given ? clk : *E.clock;  // the block's clock
   fis_trial tr[2];
   int64_t sidx[2];
   uint32_t fl[2], dm[2];
@@ -935,12 +963,21 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
     fl[t] = dm[t] = 0;
     rate[t] = vv[t] = gg[t] = rr[t] = 0.f;
     if (valid && t < nt) {
-      vv[t] = ld_hint(E.v + sidx[t], stream);
-      gg[t] = ld_hint(E.g + sidx[t], stream);
-      rr[t] = ld_hint(E.refrac + sidx[t], stream);
       fl[t] = ld_hint(E.flags + sidx[t], stream);
-      rate[t] = ld_hint(E.rates + sidx[t], stream);
-      if (!kTape && K > 1) dm[t] = ld_hint(E.kicks + sidx[t], stream);
+      if (pre) {  // this thread's own async copies: visible to it once waited for
+        cp_async_wait_all();
+        vv[t] = pre[(0 * 2 + t) * kUpdThreads + threadIdx.x];
+        gg[t] = pre[(1 * 2 + t) * kUpdThreads + threadIdx.x];
+        rr[t] = pre[(2 * 2 + t) * kUpdThreads + threadIdx.x];
+        rate[t] = pre[(3 * 2 + t) * kUpdThreads + threadIdx.x];
+        if (!kTape && K > 1) dm[t] = __float_as_uint(pre[(4 * 2 + t) * kUpdThreads + threadIdx.x]);
+      } else {
+        vv[t] = ld_hint(E.v + sidx[t], stream);
+        gg[t] = ld_hint(E.g + sidx[t], stream);
+        rr[t] = ld_hint(E.refrac + sidx[t], stream);
+        rate[t] = ld_hint(E.rates + sidx[t], stream);
+        if (!kTape && K > 1) dm[t] = ld_hint(E.kicks + sidx[t], stream);
+      }
     }
   }
   __syncthreads();  // the staging barrier exists before anyone waits on it
@@ -985,22 +1022,21 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
   // error for the host, waits once more for copies still writing its shared
   // memory, and skips the update, still reaching the final barrier.
   const unsigned polls = E.wait_polls ? E.wait_polls : kWaitPolls;
-  const bool staged_ok = mbar_wait(&sbar, 0, polls);
+  const bool staged_ok = mbar_wait(bar, 0, polls);
   const bool failed = __syncthreads_or(!staged_ok);
   // With `bump` the grid's last CTA advances the clock.  Each CTA counts
   // itself in here, after a barrier that every one of its threads reached
   // with the clock already read, and the CTA whose count completes the grid
   // -- by then every CTA has read the clock -- writes the next clock as it
   // ends; the count's round trip overlaps the rest of the CTA.
-  unsigned arrived = 0;
-  if (bump && threadIdx.x == 0) arrived = atomicAdd(E.done, 1u) + 1u;
+  if (count && threadIdx.x == 0) *arrived = atomicAdd(E.done, 1u) + 1u;
   if (failed) {
     // The staged lines were neither consumed nor returned to empty: the
     // host must refill the ring before it is used again.  A second wait
     // that also runs out leaves copies that may still write this CTA's
     // shared memory after it ends: FIS_ERR_STAGE_LOST, fatal for the context.
     if (threadIdx.x == 0) atomicOr(E.done + 1, (uint32_t)FIS_ERR_STAGE);
-    if (!staged_ok && !mbar_wait(&sbar, 0, polls))
+    if (!staged_ok && !mbar_wait(bar, 0, polls))
       atomicOr(E.done + 1, (uint32_t)FIS_ERR_STAGE_LOST);
   } else {
   // The staged lines are in shared memory: warp 0 returns them to empty in
@@ -1056,7 +1092,7 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
   // Every lane of a warp runs the same step loop (the choice depends on the
   // trials and on the warp's vote only), so every lane reaches each ballot.
   Staged2 in;
-  in.col = &sring[0][threadIdx.x];
+  in.col = &srow[0][threadIdx.x];
   in.mask0 = (fl[0] & (FIS_FL_SILENCED | FIS_FL_IN_OFF)) ? 0u : (kHalf ? 0x0000FFFFu : 0xFFFFFFFFu);
   in.mask1 = (fl[1] & (FIS_FL_SILENCED | FIS_FL_IN_OFF)) ? 0u : (kHalf ? 0xFFFF0000u : 0xFFFFFFFFu);
   // A trial slot that does not run is inert in the lanes it shares (never
@@ -1178,15 +1214,103 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
   // the grid is, before the next scatter, a later kernel, adds into them.
   if (threadIdx.x < kWarp) bulk_wait_all();
   }  // the staged input arrived
+}
 
+// The grid's last CTA to count itself in writes the next clock.
+__device__ __forceinline__ void clock_bump(const fis_engine& E, const int bump,
+                                           const unsigned arrived, const fis_clock& ck,
+                                           const int K) {
   if (bump && threadIdx.x == 0 && arrived == gridDim.x * gridDim.y) {
+    const int L = E.p.lag;
     *E.done = 0u;
     fis_clock next;
-    next.step = t0 + K;
+    next.step = ck.step + K;
     next.slot = wrap(ck.slot + K, L);
     next.slot2 = wrap(ck.slot2 + K, 2 * L);
     *E.clock = next;
   }
+}
+
+// One tile per CTA: grid (tiles, trial pairs).
+template <bool kTape, bool kHalf>
+__global__ void __launch_bounds__(kUpdThreads, 4)
+k_update(const fis_engine E, const int b0, const int nb, const int K,
+         int32_t* __restrict__ ring, float* __restrict__ spikes_out,
+         const int bump, const float unit,  // unit: 1.0f (see addp)
+         const fis_clock clk, const int clk_given) {
+  // The block's delayed input, a column per thread (per trial for int32):
+  // staged so the step loop stays rolled (a compact body that fits the
+  // instruction cache) and can index it by step.
+  __shared__ __align__(128) int32_t sring[FIS_MAX_BLOCK][StagedRow<kHalf>::kWords];
+  __shared__ __align__(16) uint32_t szero[kTile];                  // source of the clearing
+  __shared__ uint32_t sbal[2][kUpdThreads / kWarp][FIS_MAX_BLOCK]; // raster words per step
+  __shared__ __align__(8) uint64_t sbar;                           // staging barrier
+  if (threadIdx.x < kWarp) stage_tile<kHalf>(E, ring, nb, K, blockIdx.y, blockIdx.x, sring, &sbar);
+  const fis_clock ck = clk_given ? clk : *E.clock;  // the block's clock
+  unsigned arrived = 0;
+  update_tile<kTape, kHalf>(E, b0, nb, K, ring, spikes_out, unit, ck, blockIdx.x, sring, &sbar,
+                            szero, sbal, nullptr, bump != 0, &arrived);
+  clock_bump(E, bump, arrived, ck, K);
+}
+
+// Two tiles per CTA: grid (ceil(tiles / 2), trial pairs).  Both tiles' slots
+// are staged at entry and the second tile's state is fetched into shared
+// memory by async copies, so its loads land while the first tile's steps run
+// instead of after them.  Dynamic shared memory, laid out by PairSmem.
+template <bool kHalf>
+struct PairSmem {
+  static constexpr size_t kRing = sizeof(int32_t) * FIS_MAX_BLOCK * StagedRow<kHalf>::kWords;
+  static constexpr size_t kZero = kRing * 2;
+  static constexpr size_t kBal = kZero + sizeof(uint32_t) * kTile;
+  static constexpr size_t kBar = kBal + sizeof(uint32_t) * 2 * (kUpdThreads / kWarp) * FIS_MAX_BLOCK;
+  static constexpr size_t kPre = kBar + sizeof(uint64_t) * 2;
+  static constexpr size_t kBytes = kPre + sizeof(float) * 5 * 2 * kUpdThreads;
+};
+
+template <bool kHalf>
+__global__ void __launch_bounds__(kUpdThreads, 4)
+k_update_pair(const fis_engine E, const int b0, const int nb, const int K,
+              int32_t* __restrict__ ring, float* __restrict__ spikes_out,
+              const int bump, const float unit, const fis_clock clk, const int clk_given) {
+  extern __shared__ __align__(128) uint8_t dsm[];
+  using S = PairSmem<kHalf>;
+  auto sring = reinterpret_cast<int32_t(*)[FIS_MAX_BLOCK][StagedRow<kHalf>::kWords]>(dsm);
+  uint32_t* szero = reinterpret_cast<uint32_t*>(dsm + S::kZero);
+  auto sbal = reinterpret_cast<uint32_t(*)[kUpdThreads / kWarp][FIS_MAX_BLOCK]>(dsm + S::kBal);
+  uint64_t* sbar = reinterpret_cast<uint64_t*>(dsm + S::kBar);
+  float* pre = reinterpret_cast<float*>(dsm + S::kPre);
+  const int n = E.n;
+  const int pp = blockIdx.y;
+  const int tile0 = blockIdx.x * 2;
+  const bool two = tile0 + 1 < ring_row(n) / kTile;
+  if (threadIdx.x < kWarp) {
+    stage_tile<kHalf>(E, ring, nb, K, pp, tile0, sring[0], &sbar[0]);
+    if (two) stage_tile<kHalf>(E, ring, nb, K, pp, tile0 + 1, sring[1], &sbar[1]);
+  }
+  if (two) {
+    const uint64_t stream = policy_stream();
+    const int nt = (2 * pp + 1 < nb) ? 2 : 1;
+    const int i = (tile0 + 1) * kTile + threadIdx.x;
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      if (i < n && t < nt) {
+        const int64_t si = (int64_t)(b0 + 2 * pp + t) * n + i;
+        const void* src[5] = {E.v + si, E.g + si, E.refrac + si, E.rates + si, E.kicks + si};
+#pragma unroll
+        for (int a = 0; a < 5; ++a)
+          cp_async4(&pre[(a * 2 + t) * kUpdThreads + threadIdx.x], src[a], stream);
+      }
+    }
+    cp_async_commit();
+  }
+  const fis_clock ck = clk_given ? clk : *E.clock;
+  unsigned arrived = 0;
+  update_tile<false, kHalf>(E, b0, nb, K, ring, spikes_out, unit, ck, tile0, sring[0], &sbar[0],
+                            szero, sbal, nullptr, bump != 0, &arrived);
+  if (two)
+    update_tile<false, kHalf>(E, b0, nb, K, ring, spikes_out, unit, ck, tile0 + 1, sring[1],
+                              &sbar[1], szero, sbal, pre, false, &arrived);
+  clock_bump(E, bump, arrived, ck, K);
 }
 
 // ---------------------------------------------------------------------------
@@ -1333,6 +1457,7 @@ int fis_check(const fis_engine* e) {
   if (e->scat_ctas < 0 || e->drive_ctas < 0 || e->scat_ctas > 256 || e->drive_ctas > 256)
     return FIS_E_ARG;
   if (e->update_streams < 0 || e->update_streams > 2) return FIS_E_ARG;
+  if (e->update_tiles < 0 || e->update_tiles > 2) return FIS_E_ARG;
   if (!aligned16(e->edges)) return FIS_E_ALIGN;
   return FIS_OK;
 }
@@ -1435,6 +1560,24 @@ int update_block(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, i
   if (clk) c = *clk;
   const int given = clk ? 1 : 0;
   const int bp = bump ? 1 : 0;
+  if (!e->vstim && e->ring16 && k_steps > 1 && e->update_tiles == 2) {
+    // two tiles per CTA: the attribute for its dynamic shared memory is set
+    // once per device
+    static int sized[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !sized[dev]) {
+      const cudaError_t err = cudaFuncSetAttribute(
+          k_update_pair<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+          (int)PairSmem<true>::kBytes);
+      if (err != cudaSuccess) return (int)err;
+      sized[dev] = 1;
+    }
+    const dim3 pgrid((ring_row(e->n) / kTile + 1) / 2, (nb + 1) / 2);
+    k_update_pair<true><<<pgrid, kUpdThreads, PairSmem<true>::kBytes, st>>>(
+        *e, b0, nb, k_steps, ring, spikes_out, bp, 1.0f, c, given);
+    return launch_status();
+  }
   if (e->vstim) {
     if (e->ring16)
       k_update<true, true><<<ugrid, kUpdThreads, 0, st>>>(*e, b0, nb, k_steps, ring, spikes_out,

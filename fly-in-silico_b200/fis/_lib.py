@@ -17,7 +17,7 @@ PKG = Path(__file__).resolve().parent
 LIB_NAME = "libfis_b200.so"
 LIB_PATH = PKG / LIB_NAME
 
-FIS_ABI_VERSION = 7
+FIS_ABI_VERSION = 8
 FIS_MAX_BLOCK = 20
 FIS_NOALLOC_RING_INTS = 3 << 20
 REF_EV_ABI = 3
@@ -83,7 +83,8 @@ class EngineDesc(ctypes.Structure):
                 ("wait_polls", ctypes.c_uint32), ("inject_stall", ctypes.c_uint32),
                 ("raster", ctypes.c_int32), ("scatter_mode", ctypes.c_int32),
                 ("scat_ctas", ctypes.c_int32), ("drive_ctas", ctypes.c_int32),
-                ("update_streams", ctypes.c_int32), ("p", LifParams)]
+                ("update_streams", ctypes.c_int32), ("update_tiles", ctypes.c_int32),
+                ("pad3_", ctypes.c_int32), ("p", LifParams)]
 
 
 _lib = None

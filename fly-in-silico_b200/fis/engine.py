@@ -88,7 +88,7 @@ class Core:
     def __init__(self, conn: Connectome, batch: int, params=None, device="cuda",
                  group=None, chunk=None, max_block=_lib.FIS_MAX_BLOCK, ring=None,
                  overlap=True, raster=True, scatter_mode=None, scat_ctas=0, drive_ctas=0,
-                 update_streams=1):
+                 update_streams=1, update_tiles=None):
         self.device = require_cuda(device)
         self.lib = _lib.load()
         conn.check_bounds()
@@ -199,9 +199,10 @@ class Core:
         d.ring16 = 1 if self.ring16 else 0
         d.raster = 1 if self.raster else 0
         d.p = self.P
-        self.set_launch(scatter_mode, scat_ctas, drive_ctas, update_streams)
+        self.set_launch(scatter_mode, scat_ctas, drive_ctas, update_streams, update_tiles)
 
-    def set_launch(self, scatter_mode=None, scat_ctas=0, drive_ctas=0, update_streams=1):
+    def set_launch(self, scatter_mode=None, scat_ctas=0, drive_ctas=0, update_streams=1,
+                   update_tiles=None):
         """Phase A's launch shape (exact: it changes scheduling, never sums).
 
         ``scatter_mode`` 0: a warp walks one work item (spike, row chunk) at a
@@ -210,15 +211,21 @@ class Core:
         ``drive_ctas``: scattering and drive CTAs per 8 SMs (0: the library's
         default for the mode).  ``update_streams`` 2: in the overlapped native
         loop, consecutive updates (of different trial groups) alternate
-        between two streams.
+        between two streams.  ``update_tiles`` 2: each update CTA takes two
+        256-neuron tiles and fetches the second one's input while the first
+        one's steps run (None: ``FIS_UPDATE_TILES``, else 2).
         """
         if scatter_mode is None:
             scatter_mode = int(os.environ.get("FIS_SCATTER_MODE", "1"))
+        if update_tiles is None:
+            update_tiles = int(os.environ.get("FIS_UPDATE_TILES", "2"))
         d = self.desc
         d.scatter_mode, d.scat_ctas, d.drive_ctas = (int(scatter_mode), int(scat_ctas),
                                                      int(drive_ctas))
         d.update_streams = int(update_streams)
+        d.update_tiles = int(update_tiles)
         _lib.check(self.lib.fis_check(ctypes.byref(d)), "fis_check")
+        self.update_tiles = int(update_tiles)
         self.scatter_mode, self.scat_ctas, self.drive_ctas = (int(scatter_mode), int(scat_ctas),
                                                                int(drive_ctas))
         self.update_streams = int(update_streams)

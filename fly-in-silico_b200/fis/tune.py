@@ -21,11 +21,13 @@ Tunables (all exact: they change scheduling and storage, never results):
 * ``update_streams`` -- 1, or 2: consecutive updates (of different trial
   groups, so independent) alternate between two streams and overlap their
   tails.
+* ``update_tiles`` -- 256-neuron tiles per update CTA, 1 or 2 (the second
+  tile's input is fetched while the first one's steps run).
 
 The block length stays the delay lag (20 steps), the longest that keeps the
 steps of a block independent.  The search is coordinate-wise: group x ring at
 the default launch, then scatter mode x chunk at the best of those, then the
-phase-A grid, then the update streams.  Each candidate runs a short seeded trial mix on a scratch
+phase-A grid, then the update streams and tiles per CTA.  Each candidate runs a short seeded trial mix on a scratch
 engine and is timed with CUDA events; the winner is stored in a JSON cache
 (``FIS_TUNE_CACHE`` or ``~/.cache/fis/tune.json``).
 """
@@ -43,7 +45,7 @@ from .connectome import Connectome
 from .engine import Core
 
 KEYS = ("group", "ring", "scatter_mode", "chunk", "scat_ctas", "drive_ctas",
-        "update_streams")
+        "update_streams", "update_tiles")
 
 
 def cache_path() -> Path:
@@ -53,7 +55,7 @@ def cache_path() -> Path:
 
 def _key(conn: Connectome, batch: int) -> str:
     name = torch.cuda.get_device_name() if torch.cuda.is_available() else "cpu"
-    return "%s|n=%d|e=%d|b=%d|v4" % (name, conn.n, conn.nnz, batch)
+    return "%s|n=%d|e=%d|b=%d|v5" % (name, conn.n, conn.nnz, batch)
 
 
 def load_cache() -> dict:
@@ -133,7 +135,7 @@ def tune(conn: Connectome, batch: int, params=None, groups=None, rings=None, mod
         c = core_for(cand["ring"], cand["chunk"])
         c.set_group(cand["group"])
         c.set_launch(cand["scatter_mode"], cand["scat_ctas"], cand["drive_ctas"],
-                     cand["update_streams"])
+                     cand["update_streams"], cand["update_tiles"])
         ms = _time(c, steps, reps)
         results.append(dict(cand, ms_per_step=ms))
         if verbose:
@@ -144,7 +146,8 @@ def tune(conn: Connectome, batch: int, params=None, groups=None, rings=None, mod
         return {k: min(results, key=lambda r: r["ms_per_step"])[k] for k in KEYS}
 
     best = {"group": groups[0], "ring": rings[0], "scatter_mode": modes[0],
-            "chunk": base_chunk, "scat_ctas": 0, "drive_ctas": 0, "update_streams": 1}
+            "chunk": base_chunk, "scat_ctas": 0, "drive_ctas": 0, "update_streams": 1,
+            "update_tiles": 2}
     # 1. batch width x ring layout at the default launch
     for ring in rings:
         for g in groups:
@@ -169,6 +172,12 @@ def tune(conn: Connectome, batch: int, params=None, groups=None, rings=None, mod
             cand = dict(best, group=g, update_streams=2)
             if not seen(cand):
                 trial(cand)
+    best = best_so_far()
+    # 5. one or two tiles per update CTA
+    for tiles in (1, 2):
+        cand = dict(best, update_tiles=tiles)
+        if not seen(cand):
+            trial(cand)
     cores.clear()
     torch.cuda.empty_cache()
     win = min(results, key=lambda r: r["ms_per_step"])
@@ -189,4 +198,5 @@ def core_kwargs(best: dict) -> dict:
     return {"group": best["group"], "chunk": best.get("chunk"), "ring": best.get("ring"),
             "scatter_mode": best.get("scatter_mode"), "scat_ctas": best.get("scat_ctas", 0),
             "drive_ctas": best.get("drive_ctas", 0),
-            "update_streams": best.get("update_streams", 1)}
+            "update_streams": best.get("update_streams", 1),
+            "update_tiles": best.get("update_tiles")}

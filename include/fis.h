@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define FIS_ABI_VERSION 7
+#define FIS_ABI_VERSION 8
 
 /* Largest number of steps one block may advance (registers per thread). */
 #define FIS_MAX_BLOCK 20
@@ -177,6 +177,12 @@ typedef struct fis_engine {
   int32_t update_streams;  /* fis_advance_overlap: 2 = consecutive updates
                               (of different trial groups) alternate between
                               the caller's stream and a second one; else 1 */
+  int32_t update_tiles;    /* 256-neuron tiles per update CTA: 2 = each CTA
+                              stages both tiles' slots at entry and fetches
+                              the second tile's state into shared memory
+                              while the first one's steps run (paired int16
+                              ring, Philox drive, blocks of 2+ steps); else 1 */
+  int32_t pad3_;
   fis_lif_params p;
 } fis_engine;
 

@@ -111,7 +111,9 @@ def test_server_latency_stats_and_budget():
 @pytest.mark.parametrize("ring", ["int16", "int32"])
 @pytest.mark.parametrize("scatter_mode", [0, 1])
 @pytest.mark.parametrize("update_streams,group", [(1, 2), (2, 2), (2, 3)])
-def test_overlapped_advance_equals_sequential(ring, scatter_mode, update_streams, group):
+@pytest.mark.parametrize("update_tiles", [1, 2])
+def test_overlapped_advance_equals_sequential(ring, scatter_mode, update_streams, group,
+                                              update_tiles):
     """Scatter/update overlap on two rings (updates on one or two streams,
     an even and an odd number of trial groups) gives the one-ring result, bit
     for bit."""
@@ -123,7 +125,7 @@ def test_overlapped_advance_equals_sequential(ring, scatter_mode, update_streams
     got = []
     for overlap in (False, True):
         core = Core(c, 7, group=group, ring=ring, overlap=overlap, scatter_mode=scatter_mode,
-                    update_streams=update_streams)
+                    update_streams=update_streams, update_tiles=update_tiles)
         counts = Batch(c, 7, core=core).run(sp)
         got.append((counts, core.v.cpu().numpy(), core.g.cpu().numpy(),
                     core.refrac.cpu().numpy(), core.step))

@@ -28,7 +28,7 @@ def raster_rows(core, first, last):
     return out
 
 
-def make_engine(name, graphs=False, group=None, ring=None, scatter_mode=None):
+def make_engine(name, graphs=False, group=None, ring=None, scatter_mode=None, update_tiles=None):
     from fis import sim
 
     sc = S.SCENARIOS[name]
@@ -36,8 +36,8 @@ def make_engine(name, graphs=False, group=None, ring=None, scatter_mode=None):
     eng = sim.build_engine(weights=conn, silenced=S.silenced(sc), params=sc["params"],
                            batch=sc["batch"], seed=sc["seed"], no_refractory=S.driven(sc),
                            graphs=graphs, group=group, ring=ring)
-    if scatter_mode is not None:
-        eng.core.set_launch(scatter_mode)
+    if scatter_mode is not None or update_tiles is not None:
+        eng.core.set_launch(scatter_mode, update_tiles=update_tiles)
     return sc, eng
 
 
@@ -97,12 +97,15 @@ def test_tape_driven_core_matches_reference(name, golden):
 @pytest.mark.parametrize("name", SMALL)
 @pytest.mark.parametrize("group", [None, 1, 2])
 @pytest.mark.parametrize("ring", ["int16", "int32"])
-@pytest.mark.parametrize("scatter_mode", [0, 1])
-def test_blocked_stepping_matches_reference(name, group, ring, scatter_mode, golden):
+@pytest.mark.parametrize("scatter_mode,update_tiles", [(0, 1), (1, 1), (1, 2)])
+def test_blocked_stepping_matches_reference(name, group, ring, scatter_mode, update_tiles,
+                                            golden):
     """Blocks of up to 20 fused steps, split only where the masks change; both
-    scatter forms (a warp per work item, a warp per 32 items)."""
+    scatter forms (a warp per work item, a warp per 32 items) and one or two
+    tiles per update CTA."""
     z = golden(name)
-    sc, eng = make_engine(name, group=group, ring=ring, scatter_mode=scatter_mode)
+    sc, eng = make_engine(name, group=group, ring=ring, scatter_mode=scatter_mode,
+                          update_tiles=update_tiles)
     assert eng.core.ring16 == (ring == "int16")
     core = eng.core
     core.rates.copy_(torch.from_numpy(S.rates_matrix(sc)))
@@ -124,11 +127,11 @@ def test_blocked_stepping_matches_reference(name, group, ring, scatter_mode, gol
     assert final_state_equal(eng, z) == []
 
 
-@pytest.mark.parametrize("scatter_mode", [0, 1])
-def test_full_size_config0_matches_reference(scatter_mode, golden):
+@pytest.mark.parametrize("scatter_mode,update_tiles", [(0, 1), (1, 1), (1, 2)])
+def test_full_size_config0_matches_reference(scatter_mode, update_tiles, golden):
     """138,639 neurons, 15.09 M edges, 1,000 steps in 20-step blocks."""
     z = golden("full_cfg0")
-    sc, eng = make_engine("full_cfg0", scatter_mode=scatter_mode)
+    sc, eng = make_engine("full_cfg0", scatter_mode=scatter_mode, update_tiles=update_tiles)
     core = eng.core
     core.rates.copy_(torch.from_numpy(S.rates_matrix(sc)))
     rows = []
