@@ -213,12 +213,14 @@ class Core:
         loop, consecutive updates (of different trial groups) alternate
         between two streams.  ``update_tiles`` 2: each update CTA takes two
         256-neuron tiles and fetches the second one's input while the first
-        one's steps run (None: ``FIS_UPDATE_TILES``, else 2).
+        one's steps run (None: ``FIS_UPDATE_TILES``, else 1; two measured
+        slower on the bench: half the CTAs, and their shared memory leaves the
+        SM little L1).
         """
         if scatter_mode is None:
             scatter_mode = int(os.environ.get("FIS_SCATTER_MODE", "1"))
         if update_tiles is None:
-            update_tiles = int(os.environ.get("FIS_UPDATE_TILES", "2"))
+            update_tiles = int(os.environ.get("FIS_UPDATE_TILES", "1"))
         d = self.desc
         d.scatter_mode, d.scat_ctas, d.drive_ctas = (int(scatter_mode), int(scat_ctas),
                                                      int(drive_ctas))

@@ -147,7 +147,7 @@ def tune(conn: Connectome, batch: int, params=None, groups=None, rings=None, mod
 
     best = {"group": groups[0], "ring": rings[0], "scatter_mode": modes[0],
             "chunk": base_chunk, "scat_ctas": 0, "drive_ctas": 0, "update_streams": 1,
-            "update_tiles": 2}
+            "update_tiles": 1}
     # 1. batch width x ring layout at the default launch
     for ring in rings:
         for g in groups:
