@@ -61,6 +61,7 @@ class Reply:
     finished: float
     trial_steps: int
     slots: list = field(default_factory=list)
+    released: float = 0.0            # its slots were freed (its trials had all ended)
 
     @property
     def latency(self):
@@ -106,6 +107,8 @@ class Server:
         # end): new arrivals wait at most this long for admission
         self.advance_steps = max(1, int(advance_steps))
         self._in_flight = None                # event after the previous turn's work
+        self._copy_stream = None              # recordings of retired requests go out here
+        self._retiring = []                   # retired, their recordings on the way out
         self.clock0 = time.perf_counter()
 
     # --- host side --------------------------------------------------------
@@ -151,22 +154,57 @@ class Server:
         return admitted
 
     def _retire(self):
+        """Retire the requests whose trials end with the stretch just enqueued.
+
+        Their slots are freed at once (a new occupant's load runs after that
+        stretch in stream order), while their recordings are reduced and
+        copied to pinned host memory on a copy stream that waits only for that
+        stretch, so the device keeps running; ``_finish`` turns them into
+        replies once the copies have landed.
+        """
         done = [rid for rid, (_, _, end, _, _) in self.running.items() if self.core.step >= end]
-        if done:
-            self.core.check_errors()
+        if not done:
+            return done
+        dev = self.core.device
+        if self._copy_stream is None:
+            self._copy_stream = torch.cuda.Stream(dev)
+        cs = self._copy_stream
+        cs.wait_event(self._in_flight)
         for rid in done:
             req, slots, end, rec, t_adm = self.running.pop(rid)
-            bins = rec.to(torch.int16).cpu().numpy()
-            counts = rec.to(torch.int64).sum(0).cpu().numpy()
+            with torch.cuda.stream(cs):
+                bins = torch.empty(rec.shape, dtype=torch.int16, pin_memory=True)
+                counts = torch.empty(rec.shape[1], dtype=torch.int64, pin_memory=True)
+                bins.copy_(rec.to(torch.int16), non_blocking=True)
+                counts.copy_(rec.to(torch.int64).sum(0), non_blocking=True)
+                err = self.core.errors_async()
+                landed = torch.cuda.Event()
+                landed.record(cs)
+            rec.record_stream(cs)
             for b in slots:
                 self.core.trials[b].start = self.core.trials[b].end = 0
                 self.batch.release(b)
                 heapq.heappush(self.free, b)
             self.core.mark_trials()
-            self.memory_used -= self.request_bytes(req)
-            self.replies.append(Reply(rid, counts, bins, req.arrival, t_adm, self.now(),
-                                      sum(int(t.steps) for t in req.trials), slots))
+            self._retiring.append((rid, req, slots, t_adm, landed, bins, counts, err, rec,
+                                   self.now()))
         return done
+
+    def _finish(self, wait=False):
+        """Replies for the retired requests whose recordings have landed."""
+        keep = []
+        for item in self._retiring:
+            rid, req, slots, t_adm, landed, bins, counts, err, rec, t_rel = item
+            if not (wait or landed.query()):
+                keep.append(item)
+                continue
+            landed.synchronize()
+            self.core.raise_errors(err)
+            self.memory_used -= self.request_bytes(req)
+            self.replies.append(Reply(rid, counts.numpy(), bins.numpy(), req.arrival, t_adm,
+                                      self.now(), sum(int(t.steps) for t in req.trials), slots,
+                                      t_rel))
+        self._retiring = keep
 
     def _active_rows(self):
         """Slots [0, hi) hold every running trial; launches stop at hi."""
@@ -210,7 +248,7 @@ class Server:
         pending = sorted(requests, key=lambda r: r.arrival)
         self.clock0 = time.perf_counter()
         i = 0
-        while i < len(pending) or self.queue or self.running:
+        while i < len(pending) or self.queue or self.running or self._retiring:
             now = self.now()
             while i < len(pending) and (not realtime or pending[i].arrival <= now):
                 if not realtime:
@@ -221,6 +259,9 @@ class Server:
             if self.running:
                 self.step_block()
                 self._retire()
+                self._finish()
+            elif self._retiring:
+                self._finish(wait=True)
             elif i < len(pending):
                 time.sleep(min(max_idle_wait, max(0.0, pending[i].arrival - self.now())))
         torch.cuda.synchronize(self.core.device)

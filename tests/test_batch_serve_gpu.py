@@ -85,7 +85,7 @@ def test_request_same_alone_and_in_mix():
     replies = Server(c, capacity=8, group=4).run(mix, realtime=False)
     got = {r.rid: r for r in replies}
     t_mix = got[1]
-    assert t_mix.admitted >= got[0].finished  # it waited for request 0's slots
+    assert t_mix.admitted >= got[0].released  # it waited for request 0's slots
     assert np.array_equal(t_mix.counts, alone[0].counts)
     assert np.array_equal(t_mix.bins, alone[0].bins)
     # and against the oracle, trial by trial summed
