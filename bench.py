@@ -84,8 +84,8 @@ def uneven_run(conn):
     from fis.batch import Batch, random_specs
     from fis.tune import core_kwargs, tune
 
-    best = tune(conn, 256)
     specs = random_specs(conn.n, 256, SPEC_SEED + 7, (500, 20000))
+    best = tune(conn, 256, specs=specs, tag="uneven-mix-%d" % (SPEC_SEED + 7))
     b = Batch(conn, 256, **core_kwargs(best))
     b.run(specs[:8])  # warm the allocations
     torch.cuda.synchronize()
@@ -430,7 +430,7 @@ def main():
     conn = C.synthetic(seed=CONN_SEED)
     specs = random_specs(conn.n, args.trials, SPEC_SEED + 1000 * rank, args.sim_steps)
     if args.group is None:
-        best = tune(conn, args.trials)
+        best = tune(conn, args.trials, specs=specs, tag="bench-mix-%d" % (SPEC_SEED + 1000 * rank))
     else:
         best = {"group": args.group, "chunk": None, "ring": None, "scatter_mode": None,
                 "scat_ctas": 0, "drive_ctas": 0, "update_streams": 1, "update_tiles": None,

@@ -100,11 +100,27 @@ def default_groups(batch):
     return sorted({g for g in (1, 2, 4, 8, 16, 32, 64, 128, 256) if g <= batch} | {batch})
 
 
+def _load_specs(core: Core, specs):
+    """The caller's own trials (``fis.batch.TrialSpec``) in the scratch core,
+    running past every candidate's steps."""
+    from .batch import Batch
+
+    Batch(core.conn, core.batch, core=core).load(list(range(len(specs))), specs)
+    for b in range(core.batch):
+        core.trials[b].end = 2 ** 62
+    core.mark_trials()
+
+
 def tune(conn: Connectome, batch: int, params=None, groups=None, rings=None, modes=(1, 0),
-         chunks=None, grids=None, steps=1000, reps=2, use_cache=True, verbose=False) -> dict:
+         chunks=None, grids=None, steps=1000, reps=2, use_cache=True, verbose=False,
+         specs=None, tag="mix") -> dict:
     """Best launch shape ``{group, ring, scatter_mode, chunk, scat_ctas,
-    drive_ctas, ms_per_step, candidates}`` for this connectome and batch."""
-    key = _key(conn, batch)
+    drive_ctas, update_streams, update_tiles, ms_per_step, candidates}`` for
+    this connectome and batch.  ``specs``: time the candidates on these trials
+    (``batch`` of them) instead of the seeded 2 % mix -- the choices differ by a
+    few percent, so the workload that will run is the one to tune on; ``tag``
+    names it in the cache key."""
+    key = _key(conn, batch) + "|" + str(tag)
     cache = load_cache() if use_cache else {}
     if key in cache:
         return cache[key]
@@ -124,7 +140,10 @@ def tune(conn: Connectome, batch: int, params=None, groups=None, rings=None, mod
             torch.cuda.empty_cache()
             c = Core(conn, batch, params=params, chunk=chunk, group=groups[0], ring=ring,
                      raster=False)
-            _mix(c)
+            if specs is not None:
+                _load_specs(c, specs)
+            else:
+                _mix(c)
             cores[(ring, chunk)] = c
         return cores[(ring, chunk)]
 
