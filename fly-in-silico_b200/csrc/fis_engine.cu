@@ -906,26 +906,203 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem, uint64_t
                "l"(gmem), "l"(pol)
                : "memory");
 }
-__device__ __forceinline__ void cp_async_commit() {
-  asm volatile("cp.async.commit_group;\n" ::: "memory");
-}
 __device__ __forceinline__ void cp_async_wait_all() {
-  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
+// What the prologue of an update kernel gathers for one thread's neuron in
+// the two trials of its pair, for tile_compute.
+struct TileState {
+  float v[2], g[2], r[2], vclamp[2];
+  uint32_t fl[2], dm[2];  // flags; kick steps (bit k = step k)
+  int ka[2], kb[2];       // the trial's steps of this block: [ka, kb)
+  bool runs[2];           // the trial runs in this block (uniform in the CTA)
+  bool s_prev[2];         // the neuron fired at the step before the block
+};
+
+// The K steps of one tile for both trials of pair `pp` and the epilogue:
+// state stores, raster words, spike lists and recording bins.  `srow`: the
+// staged slots (the step loop's input); `sbal`: the raster words of the
+// warp's steps.
+template <bool kTape, bool kHalf>
+__device__ __forceinline__ void tile_compute(
+    const fis_engine& E, const int b0, const int K, float* __restrict__ spikes_out,
+    const float unit, const fis_clock& ck, const int tile, const int pp,
+    int32_t (*srow)[StagedRow<kHalf>::kWords],
+    uint32_t (*sbal)[kUpdThreads / kWarp][FIS_MAX_BLOCK], const TileState& S,
+    const bool warp_driven, const int64_t (&sidx)[2]) {
+  const int n = E.n;
+  const int L = E.p.lag;
+  const int Wd = (n + kWarp - 1) / kWarp;
+  const int i = tile * kTile + threadIdx.x;
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int wib = threadIdx.x / kWarp;
+  const bool valid = i < n;
+  const bool warp_valid = (i - lane) < n;
+  const int64_t t0 = ck.step;
+  const int slot0 = ck.slot;
+  const uint64_t stream = policy_stream();
+  Pair st;
+  float vth[2], rs[2], mhold[2], vhold[2];
+#pragma unroll
+  for (int t = 0; t < 2; ++t) {
+    const bool on = S.runs[t] && valid && !(S.fl[t] & FIS_FL_FIRE_OFF);
+    vth[t] = on ? E.p.v_th : __int_as_float(0x7f800000);
+    rs[t] = (S.fl[t] & FIS_FL_NOREFRAC) ? 0.f : E.p.refrac_steps;
+    const bool hold = S.fl[t] & FIS_FL_HOLD;
+    mhold[t] = hold ? 0.f : 1.f;
+    vhold[t] = hold ? S.vclamp[t] : 0.f;
+  }
+  st.v = pk2(S.v[0], S.v[1]);
+  st.g = pk2(S.g[0], S.g[1]);
+  st.r = pk2(S.r[0], S.r[1]);
+  st.keep = pk2(S.s_prev[0] ? 0.f : 1.f, S.s_prev[1] ? 0.f : 1.f);
+  st.m_hold = pk2(mhold[0], mhold[1]);
+  st.v_hold = pk2(vhold[0], vhold[1]);
+  st.rs0 = rs[0];
+  st.rs1 = rs[1];
+  st.vth0 = vth[0];
+  st.vth1 = vth[1];
+  Consts C;
+  C.one = pk2(unit, unit);
+  C.mone = pk2(-unit, -unit);
+  C.w = pk2(E.p.w_scale, E.p.w_scale);
+  C.a_syn = pk2(E.p.a_syn, E.p.a_syn);
+  C.a_mem = pk2(E.p.a_mem, E.p.a_mem);
+  C.v_rest = pk2(E.p.v_rest, E.p.v_rest);
+  C.v_reset = pk2(E.p.v_reset, E.p.v_reset);
+
+  // Every lane of a warp runs the same step loop (the choice depends on the
+  // trials and on the warp's vote only), so every lane reaches each ballot.
+  Staged2 in;
+  in.col = &srow[0][threadIdx.x];
+  in.mask0 = (S.fl[0] & (FIS_FL_SILENCED | FIS_FL_IN_OFF)) ? 0u : (kHalf ? 0x0000FFFFu : 0xFFFFFFFFu);
+  in.mask1 = (S.fl[1] & (FIS_FL_SILENCED | FIS_FL_IN_OFF)) ? 0u : (kHalf ? 0xFFFF0000u : 0xFFFFFFFFu);
+  // A trial slot that does not run is inert in the lanes it shares (never
+  // fires, never stored), so only a trial that starts or ends inside the
+  // block needs the per-step commit of the partial loop.
+  const bool full = (!S.runs[0] || (S.ka[0] == 0 && S.kb[0] == K)) &&
+                    (!S.runs[1] || (S.ka[1] == 0 && S.kb[1] == K));
+  const bool hold_any = __any_sync(0xFFFFFFFFu, ((S.fl[0] | S.fl[1]) & FIS_FL_HOLD) != 0);
+  const int ka0 = S.runs[0] ? S.ka[0] : 0, kb0 = S.runs[0] ? S.kb[0] : 0;
+  const int ka1 = S.runs[1] ? S.ka[1] : 0, kb1 = S.runs[1] ? S.kb[1] : 0;
+  uint32_t* sb0 = sbal[0][wib];
+  uint32_t* sb1 = sbal[1][wib];
+  f2 nspk;
+  if (kTape)
+    nspk = step_loop2<true, false, kHalf, true>(st, C, E, K, ka0, kb0, ka1, kb1, 0u, 0u, in, sb0,
+                                               sb1, sidx[0], sidx[1], valid);
+  else if (!full)
+    nspk = step_loop2<false, true, kHalf, true>(st, C, E, K, ka0, kb0, ka1, kb1, S.dm[0], S.dm[1],
+                                               in, sb0, sb1, sidx[0], sidx[1], valid);
+  else if (E.raster && warp_driven)
+    nspk = step_loop2<false, true, kHalf, false>(st, C, E, K, 0, K, 0, K, S.dm[0], S.dm[1], in,
+                                                sb0, sb1, sidx[0], sidx[1], valid);
+  else if (E.raster)
+    nspk = step_loop2<false, false, kHalf, false>(st, C, E, K, 0, K, 0, K, 0u, 0u, in, sb0, sb1,
+                                                 sidx[0], sidx[1], valid);
+  else if (hold_any && warp_driven)
+    nspk = step_loop2<false, true, kHalf, false, false>(st, C, E, K, 0, K, 0, K, S.dm[0],
+                                                       S.dm[1], in, sb0, sb1, sidx[0], sidx[1],
+                                                       valid);
+  else if (hold_any)
+    nspk = step_loop2<false, false, kHalf, false, false>(st, C, E, K, 0, K, 0, K, 0u, 0u, in,
+                                                        sb0, sb1, sidx[0], sidx[1], valid);
+  else if (warp_driven)  // no held lane: the hold is left out (see lif_step2)
+    nspk = step_loop2<false, true, kHalf, false, false, false>(
+        st, C, E, K, 0, K, 0, K, S.dm[0], S.dm[1], in, sb0, sb1, sidx[0], sidx[1], valid);
+  else
+    nspk = step_loop2<false, false, kHalf, false, false, false>(
+        st, C, E, K, 0, K, 0, K, 0u, 0u, in, sb0, sb1, sidx[0], sidx[1], valid);
+  // Without the full raster only the last step's words are kept (the next
+  // block reads them for the refractory reset); the partial and tape loops
+  // always store every step.
+  // The last step's words are the warp's ballots of keep == 0, which every
+  // lane holds: lane 0 stores them directly.
+  const bool only_last = !E.raster && full && !kTape;
+  if (only_last) {
+    float k0, k1;
+    up2(st.keep, k0, k1);
+    const uint32_t w0 = __ballot_sync(0xFFFFFFFFu, k0 == 0.f);
+    const uint32_t w1 = __ballot_sync(0xFFFFFFFFu, k1 == 0.f);
+    if (lane == 0 && warp_valid) {
+      const int sl = slot0 + K - 1 < L ? slot0 + K - 1 : slot0 + K - 1 - L;
+      const int64_t wrow = (int64_t)(b0 + 2 * pp) * Wd + (i >> 5);
+      if (S.runs[0]) E.bits[wrow * L + sl] = w0;
+      if (S.runs[1]) E.bits[(wrow + Wd) * L + sl] = w1;
+    }
+  } else {
+    __syncwarp();
+  }
+
+  float ov[2], og[2], orr[2], okeep[2], ospk[2];
+  up2(st.v, ov[0], ov[1]);
+  up2(st.g, og[0], og[1]);
+  up2(st.r, orr[0], orr[1]);
+  up2(st.keep, okeep[0], okeep[1]);
+  up2(nspk, ospk[0], ospk[1]);
+  // Addresses and trial fields are derived again here rather than kept live
+  // through the step loop (its register budget); the spike path reloads
+  // what it needs from L1.
+#pragma unroll
+  for (int t = 0; t < 2; ++t) {
+    if (!S.runs[t]) continue;
+    const int b = b0 + 2 * pp + t;
+    const int64_t si = (int64_t)b * n + i;
+    // the raster words of the K steps into the ring of the last L steps
+    if (!only_last && lane < K && warp_valid) {
+      const int sl = slot0 + lane < L ? slot0 + lane : slot0 + lane - L;
+      E.bits[((int64_t)b * Wd + (i >> 5)) * L + sl] = sbal[t][wib][lane];
+    }
+    if (valid) {
+      st_hint(E.v + si, ov[t], stream);
+      st_hint(E.g + si, og[t], stream);
+      st_hint(E.refrac + si, orr[t], stream);
+      if (spikes_out) spikes_out[si] = (okeep[t] == 0.f) ? 1.f : 0.f;
+    }
+    // Spike lists and recording for the (rare) steps this neuron fired.
+    uint32_t fired = (uint32_t)ospk[t];  // bit j is step K-1-j
+    if (fired) {
+      const int B = E.batch;
+      const fis_trial trl = E.trials[b];
+      const uint32_t flb = E.flags[si];
+      const int nch = (int)E.nchunks[i];
+      int32_t* const recb = (trl.rec >= 0 && trl.rec < E.n_recs) ? E.recs[trl.rec] : nullptr;
+      const bool out_on = !(flb & (FIS_FL_OUT_OFF | FIS_FL_SILENCED));
+      const int slot20 = ck.slot2;
+      const int64_t own0 = t0 - trl.start;
+      while (fired) {
+        const int k = K - __ffs(fired);
+        fired &= fired - 1;
+        const int sl = slot0 + k < L ? slot0 + k : slot0 + k - L;
+        const int sl2 = slot20 + k < 2 * L ? slot20 + k : slot20 + k - 2 * L;
+        if ((out_on || k == K - 1) && nch > 0) {
+          const int32_t pos = atomicAdd(E.list_len + (int64_t)sl2 * B + b, nch);
+          uint32_t* dst = E.lists + ((int64_t)sl * B + b) * E.list_cap;
+          for (int q = 0; q < nch; ++q)
+            if (pos + q < E.list_cap) dst[pos + q] = ((uint32_t)i << 8) | (uint32_t)q;
+        }
+        if (recb && trl.bin_steps > 0) {
+          const int64_t own = own0 + k;
+          const int64_t bin = own < 0x7FFFFFFF ? (int64_t)((int)own / trl.bin_steps)
+                                                : own / trl.bin_steps;
+          if (bin < trl.n_bins) red_hint(recb + bin * n + i, 1, stream);
+        }
+      }
+    }
+  }
 }
 
 // One tile's update: everything but the issue of its staging copies (warp 0
 // of the CTA has issued them into `srow`, completing on `bar`) and the clock
-// bump.  `pre`: this tile's v, g, refrac, rates and kicks ([5][2][threads]),
-// prefetched into shared memory by this thread's async copies, or null to read
-// them here.  `count`: this CTA counts itself in for the clock bump (into
+// bump.  `count`: this CTA counts itself in for the clock bump (into
 // *arrived) after the staging barrier.
 template <bool kTape, bool kHalf>
 __device__ __forceinline__ void update_tile(
     const fis_engine& E, const int b0, const int nb, const int K, int32_t* __restrict__ ring,
     float* __restrict__ spikes_out, const float unit, const fis_clock& ck, const int tile,
     int32_t (*srow)[StagedRow<kHalf>::kWords], uint64_t* bar, uint32_t* szero,
-    uint32_t (*sbal)[kUpdThreads / kWarp][FIS_MAX_BLOCK], const float* pre, const bool count,
-    unsigned* arrived) {
+    uint32_t (*sbal)[kUpdThreads / kWarp][FIS_MAX_BLOCK], const bool count, unsigned* arrived) {
   const int n = E.n;
   const int L = E.p.lag;
   const int Wd = (n + kWarp - 1) / kWarp;
@@ -933,7 +1110,6 @@ __device__ __forceinline__ void update_tile(
   const int pp = blockIdx.y;    // pair of trials of the group: 2 pp, 2 pp + 1
   const int i = tile * kTile + threadIdx.x;
   const int lane = threadIdx.x & (kWarp - 1);
-  const int wib = threadIdx.x / kWarp;
   const bool valid = i < n;
   const bool warp_valid = (i - lane) < n;
   const int nt = (2 * pp + 1 < nb) ? 2 : 1;  // trials in this pair
@@ -964,20 +1140,11 @@ __device__ __forceinline__ void update_tile(
     rate[t] = vv[t] = gg[t] = rr[t] = 0.f;
     if (valid && t < nt) {
       fl[t] = ld_hint(E.flags + sidx[t], stream);
-      if (pre) {  // this thread's own async copies: visible to it once waited for
-        cp_async_wait_all();
-        vv[t] = pre[(0 * 2 + t) * kUpdThreads + threadIdx.x];
-        gg[t] = pre[(1 * 2 + t) * kUpdThreads + threadIdx.x];
-        rr[t] = pre[(2 * 2 + t) * kUpdThreads + threadIdx.x];
-        rate[t] = pre[(3 * 2 + t) * kUpdThreads + threadIdx.x];
-        if (!kTape && K > 1) dm[t] = __float_as_uint(pre[(4 * 2 + t) * kUpdThreads + threadIdx.x]);
-      } else {
-        vv[t] = ld_hint(E.v + sidx[t], stream);
-        gg[t] = ld_hint(E.g + sidx[t], stream);
-        rr[t] = ld_hint(E.refrac + sidx[t], stream);
-        rate[t] = ld_hint(E.rates + sidx[t], stream);
-        if (!kTape && K > 1) dm[t] = ld_hint(E.kicks + sidx[t], stream);
-      }
+      vv[t] = ld_hint(E.v + sidx[t], stream);
+      gg[t] = ld_hint(E.g + sidx[t], stream);
+      rr[t] = ld_hint(E.refrac + sidx[t], stream);
+      rate[t] = ld_hint(E.rates + sidx[t], stream);
+      if (!kTape && K > 1) dm[t] = ld_hint(E.kicks + sidx[t], stream);
     }
   }
   __syncthreads();  // the staging barrier exists before anyone waits on it
@@ -1059,155 +1226,23 @@ __device__ __forceinline__ void update_tile(
   }
 
   if (runs[0] || runs[1]) {
-  Pair st;
-  float vth[2], rs[2], mhold[2], vhold[2];
+    TileState S;
 #pragma unroll
-  for (int t = 0; t < 2; ++t) {
-    const bool on = runs[t] && valid && !(fl[t] & FIS_FL_FIRE_OFF);
-    vth[t] = on ? E.p.v_th : __int_as_float(0x7f800000);
-    rs[t] = (fl[t] & FIS_FL_NOREFRAC) ? 0.f : E.p.refrac_steps;
-    const bool hold = fl[t] & FIS_FL_HOLD;
-    mhold[t] = hold ? 0.f : 1.f;
-    vhold[t] = hold ? tr[t].v_clamp : 0.f;
+    for (int t = 0; t < 2; ++t) {
+      S.v[t] = vv[t];
+      S.g[t] = gg[t];
+      S.r[t] = rr[t];
+      S.vclamp[t] = tr[t].v_clamp;
+      S.fl[t] = fl[t];
+      S.dm[t] = dm[t];
+      S.ka[t] = ka[t];
+      S.kb[t] = kb[t];
+      S.runs[t] = runs[t];
+      S.s_prev[t] = s_prev[t];
+    }
+    tile_compute<kTape, kHalf>(E, b0, K, spikes_out, unit, ck, tile, pp, srow, sbal, S,
+                               warp_driven, sidx);
   }
-  st.v = pk2(vv[0], vv[1]);
-  st.g = pk2(gg[0], gg[1]);
-  st.r = pk2(rr[0], rr[1]);
-  st.keep = pk2(s_prev[0] ? 0.f : 1.f, s_prev[1] ? 0.f : 1.f);
-  st.m_hold = pk2(mhold[0], mhold[1]);
-  st.v_hold = pk2(vhold[0], vhold[1]);
-  st.rs0 = rs[0];
-  st.rs1 = rs[1];
-  st.vth0 = vth[0];
-  st.vth1 = vth[1];
-  Consts C;
-  C.one = pk2(unit, unit);
-  C.mone = pk2(-unit, -unit);
-  C.w = pk2(E.p.w_scale, E.p.w_scale);
-  C.a_syn = pk2(E.p.a_syn, E.p.a_syn);
-  C.a_mem = pk2(E.p.a_mem, E.p.a_mem);
-  C.v_rest = pk2(E.p.v_rest, E.p.v_rest);
-  C.v_reset = pk2(E.p.v_reset, E.p.v_reset);
-
-  // Every lane of a warp runs the same step loop (the choice depends on the
-  // trials and on the warp's vote only), so every lane reaches each ballot.
-  Staged2 in;
-  in.col = &srow[0][threadIdx.x];
-  in.mask0 = (fl[0] & (FIS_FL_SILENCED | FIS_FL_IN_OFF)) ? 0u : (kHalf ? 0x0000FFFFu : 0xFFFFFFFFu);
-  in.mask1 = (fl[1] & (FIS_FL_SILENCED | FIS_FL_IN_OFF)) ? 0u : (kHalf ? 0xFFFF0000u : 0xFFFFFFFFu);
-  // A trial slot that does not run is inert in the lanes it shares (never
-  // fires, never stored), so only a trial that starts or ends inside the
-  // block needs the per-step commit of the partial loop.
-  const bool full = (!runs[0] || (ka[0] == 0 && kb[0] == K)) &&
-                    (!runs[1] || (ka[1] == 0 && kb[1] == K));
-  const bool hold_any = __any_sync(0xFFFFFFFFu, ((fl[0] | fl[1]) & FIS_FL_HOLD) != 0);
-  uint32_t* sb0 = sbal[0][wib];
-  uint32_t* sb1 = sbal[1][wib];
-  f2 nspk;
-  if (kTape)
-    nspk = step_loop2<true, false, kHalf, true>(st, C, E, K, runs[0] ? ka[0] : 0, runs[0] ? kb[0] : 0,
-                                               runs[1] ? ka[1] : 0, runs[1] ? kb[1] : 0, 0u, 0u, in,
-                                               sb0, sb1, sidx[0], sidx[1], valid);
-  else if (!full)
-    nspk = step_loop2<false, true, kHalf, true>(st, C, E, K, runs[0] ? ka[0] : 0,
-                                               runs[0] ? kb[0] : 0, runs[1] ? ka[1] : 0,
-                                               runs[1] ? kb[1] : 0, dm[0], dm[1], in, sb0, sb1,
-                                               sidx[0], sidx[1], valid);
-  else if (E.raster && warp_driven)
-    nspk = step_loop2<false, true, kHalf, false>(st, C, E, K, 0, K, 0, K, dm[0], dm[1], in, sb0,
-                                                sb1, sidx[0], sidx[1], valid);
-  else if (E.raster)
-    nspk = step_loop2<false, false, kHalf, false>(st, C, E, K, 0, K, 0, K, 0u, 0u, in, sb0, sb1,
-                                                 sidx[0], sidx[1], valid);
-  else if (hold_any && warp_driven)
-    nspk = step_loop2<false, true, kHalf, false, false>(st, C, E, K, 0, K, 0, K, dm[0], dm[1], in,
-                                                       sb0, sb1, sidx[0], sidx[1], valid);
-  else if (hold_any)
-    nspk = step_loop2<false, false, kHalf, false, false>(st, C, E, K, 0, K, 0, K, 0u, 0u, in,
-                                                        sb0, sb1, sidx[0], sidx[1], valid);
-  else if (warp_driven)  // no held lane: the hold is left out (see lif_step2)
-    nspk = step_loop2<false, true, kHalf, false, false, false>(
-        st, C, E, K, 0, K, 0, K, dm[0], dm[1], in, sb0, sb1, sidx[0], sidx[1], valid);
-  else
-    nspk = step_loop2<false, false, kHalf, false, false, false>(
-        st, C, E, K, 0, K, 0, K, 0u, 0u, in, sb0, sb1, sidx[0], sidx[1], valid);
-  // Without the full raster only the last step's words are kept (the next
-  // block reads them for the refractory reset); the partial and tape loops
-  // always store every step.
-  // The last step's words are the warp's ballots of keep == 0, which every
-  // lane holds: lane 0 stores them directly.
-  const bool only_last = !E.raster && full && !kTape;
-  if (only_last) {
-    float k0, k1;
-    up2(st.keep, k0, k1);
-    const uint32_t w0 = __ballot_sync(0xFFFFFFFFu, k0 == 0.f);
-    const uint32_t w1 = __ballot_sync(0xFFFFFFFFu, k1 == 0.f);
-    if (lane == 0 && warp_valid) {
-      const int sl = slot0 + K - 1 < L ? slot0 + K - 1 : slot0 + K - 1 - L;
-      if (runs[0]) bitrow[0][sl] = w0;
-      if (runs[1]) bitrow[1][sl] = w1;
-    }
-  } else {
-    __syncwarp();
-  }
-
-  float ov[2], og[2], orr[2], okeep[2], ospk[2];
-  up2(st.v, ov[0], ov[1]);
-  up2(st.g, og[0], og[1]);
-  up2(st.r, orr[0], orr[1]);
-  up2(st.keep, okeep[0], okeep[1]);
-  up2(nspk, ospk[0], ospk[1]);
-  // Addresses and trial fields are derived again here rather than kept live
-  // through the step loop (its register budget); the spike path reloads
-  // what it needs from L1.
-#pragma unroll
-  for (int t = 0; t < 2; ++t) {
-    if (!runs[t]) continue;
-    const int b = b0 + 2 * pp + t;
-    const int64_t si = (int64_t)b * n + i;
-    // the raster words of the K steps into the ring of the last L steps
-    if (!only_last && lane < K && warp_valid) {
-      const int sl = slot0 + lane < L ? slot0 + lane : slot0 + lane - L;
-      E.bits[((int64_t)b * Wd + (i >> 5)) * L + sl] = sbal[t][wib][lane];
-    }
-    if (valid) {
-      st_hint(E.v + si, ov[t], stream);
-      st_hint(E.g + si, og[t], stream);
-      st_hint(E.refrac + si, orr[t], stream);
-      if (spikes_out) spikes_out[si] = (okeep[t] == 0.f) ? 1.f : 0.f;
-    }
-    // Spike lists and recording for the (rare) steps this neuron fired.
-    uint32_t fired = (uint32_t)ospk[t];  // bit j is step K-1-j
-    if (fired) {
-      const int B = E.batch;
-      const fis_trial trl = E.trials[b];
-      const uint32_t flb = E.flags[si];
-      const int nch = (int)E.nchunks[i];
-      int32_t* const recb = (trl.rec >= 0 && trl.rec < E.n_recs) ? E.recs[trl.rec] : nullptr;
-      const bool out_on = !(flb & (FIS_FL_OUT_OFF | FIS_FL_SILENCED));
-      const int slot20 = ck.slot2;
-      const int64_t own0 = t0 - trl.start;
-      while (fired) {
-        const int k = K - __ffs(fired);
-        fired &= fired - 1;
-        const int sl = slot0 + k < L ? slot0 + k : slot0 + k - L;
-        const int sl2 = slot20 + k < 2 * L ? slot20 + k : slot20 + k - 2 * L;
-        if ((out_on || k == K - 1) && nch > 0) {
-          const int32_t pos = atomicAdd(E.list_len + (int64_t)sl2 * B + b, nch);
-          uint32_t* dst = E.lists + ((int64_t)sl * B + b) * E.list_cap;
-          for (int q = 0; q < nch; ++q)
-            if (pos + q < E.list_cap) dst[pos + q] = ((uint32_t)i << 8) | (uint32_t)q;
-        }
-        if (recb && trl.bin_steps > 0) {
-          const int64_t own = own0 + k;
-          const int64_t bin = own < 0x7FFFFFFF ? (int64_t)((int)own / trl.bin_steps)
-                                                : own / trl.bin_steps;
-          if (bin < trl.n_bins) red_hint(recb + bin * n + i, 1, stream);
-        }
-      }
-    }
-  }
-  }  // a trial of the pair runs in this block
 
   // The clearing copies have read szero before the CTA ends (it must stay
   // valid while they read it); their writes into the ring are complete when
@@ -1249,68 +1284,339 @@ k_update(const fis_engine E, const int b0, const int nb, const int K,
   const fis_clock ck = clk_given ? clk : *E.clock;  // the block's clock
   unsigned arrived = 0;
   update_tile<kTape, kHalf>(E, b0, nb, K, ring, spikes_out, unit, ck, blockIdx.x, sring, &sbar,
-                            szero, sbal, nullptr, bump != 0, &arrived);
+                            szero, sbal, bump != 0, &arrived);
   clock_bump(E, bump, arrived, ck, K);
 }
 
-// Two tiles per CTA: grid (ceil(tiles / 2), trial pairs).  Both tiles' slots
-// are staged at entry and the second tile's state is fetched into shared
-// memory by async copies, so its loads land while the first tile's steps run
-// instead of after them.  Dynamic shared memory, laid out by PairSmem.
-template <bool kHalf>
-struct PairSmem {
-  static constexpr size_t kRing = sizeof(int32_t) * FIS_MAX_BLOCK * StagedRow<kHalf>::kWords;
-  static constexpr size_t kZero = kRing * 2;
+// Streamed tiles (paired int16 ring, Philox drive, blocks of 2+ steps): each
+// CTA takes a near-equal run of consecutive items (trial pair, tile),
+// pair-major, and pipelines them.  While item j's steps run, item j+1's input
+// is already on its way: its slots into the second of two ring buffers, its
+// trial records and raster words into the second of two small buffers, its
+// state (v, g, refrac, rates, kicks and flags of both trials) into the one
+// state buffer.  So only a CTA's first item waits for its input.
+//
+// No CTA-wide barrier: warps meet only through mbarriers, so a warp that
+// finishes an item early starts the next one.  `full[s]` completes when
+// stage s holds its item (bulk copies, TMA, counted in bytes, plus the 4-byte
+// async copies of the raster words).  `taken` completes when all 8 warps
+// have taken item j's state into registers -- and so have finished item
+// j-1, whose buffers may then be refilled.  Warp 0 waits for it and issues
+// item j+1's copies; the other warps never wait for warp 0.
+//
+// A trial's row of N neurons starts anywhere, so each state row is copied
+// from the 16-byte boundary at or below the tile's first neuron: 1040 bytes
+// of floats (kStateWords) and 272 of flags (kFlagBytes), read from an offset
+// inside.  A trial whose widened rows would reach past the end of the arrays
+// (the batch's last tile) is read directly by its threads instead.  The
+// arrays and the trial records must start on 16-byte boundaries (checked by
+// the host).
+struct StreamSmem {
+  static constexpr int kStateWords = kTile + 4;
+  static constexpr int kFlagBytes = kTile + 16;
+  static constexpr int kArrays = 5;  // v, g, refrac, rates, kicks
+  static constexpr size_t kRingStage = sizeof(int32_t) * FIS_MAX_BLOCK * kTile;
+  static constexpr size_t kState = 2 * kRingStage;
+  static constexpr size_t kFlags = kState + sizeof(uint32_t) * 2 * kArrays * kStateWords;
+  static constexpr size_t kZero = kFlags + 2 * kFlagBytes;
   static constexpr size_t kBal = kZero + sizeof(uint32_t) * kTile;
-  static constexpr size_t kBar = kBal + sizeof(uint32_t) * 2 * (kUpdThreads / kWarp) * FIS_MAX_BLOCK;
-  static constexpr size_t kPre = kBar + sizeof(uint64_t) * 2;
-  static constexpr size_t kBytes = kPre + sizeof(float) * 5 * 2 * kUpdThreads;
+  static constexpr size_t kPrev = kBal + sizeof(uint32_t) * 2 * (kUpdThreads / kWarp) * FIS_MAX_BLOCK;
+  static constexpr size_t kTrials = kPrev + sizeof(uint32_t) * 2 * 2 * (kUpdThreads / kWarp);
+  static constexpr size_t kBar = kTrials + sizeof(fis_trial) * 2 * 2;
+  static constexpr size_t kClock = kBar + sizeof(uint64_t) * 3;  // full[2], taken
+  static constexpr size_t kAbort = kClock + sizeof(fis_clock);
+  static constexpr size_t kBytes = kAbort + 16;
+};
+static_assert(StreamSmem::kFlags % 16 == 0 && StreamSmem::kZero % 16 == 0 &&
+                  StreamSmem::kTrials % 16 == 0 && sizeof(fis_trial) % 16 == 0 &&
+                  StreamSmem::kBar % 8 == 0 && StreamSmem::kClock % 8 == 0,
+              "bulk copy destinations on 16-byte boundaries, barriers on 8");
+
+// Where item `item` of the group lies.  first[t]: element index of the
+// tile's first neuron in trial t's row of the [B][N] arrays; ofs/ofb: floats
+// and flag bytes from the 16-byte boundary below it; direct: read by the
+// threads, not staged (also for a trial slot the pair does not have).
+struct ItemGeo {
+  int pp, tile, nt;
+  int64_t first[2];
+  int ofs[2], ofb[2];
+  bool direct[2];
 };
 
-template <bool kHalf>
+__device__ __forceinline__ ItemGeo item_geo(const fis_engine& E, const int b0, const int nb,
+                                            const int ntiles, const int item) {
+  ItemGeo G;
+  G.pp = item / ntiles;
+  G.tile = item - G.pp * ntiles;
+  G.nt = (2 * G.pp + 1 < nb) ? 2 : 1;
+  const int64_t total = (int64_t)E.batch * E.n;
+#pragma unroll
+  for (int t = 0; t < 2; ++t) {
+    const int64_t f = (int64_t)(b0 + 2 * G.pp + (t < G.nt ? t : 0)) * E.n + G.tile * kTile;
+    G.first[t] = f;
+    G.ofs[t] = (int)(f & 3);
+    G.ofb[t] = (int)(f & 15);
+    G.direct[t] = t >= G.nt || f - G.ofs[t] + StreamSmem::kStateWords > total ||
+                  f - G.ofb[t] + StreamSmem::kFlagBytes > total;
+  }
+  return G;
+}
+
+__device__ __forceinline__ unsigned item_bytes(const ItemGeo& G, const int K) {
+  unsigned b = (unsigned)K * kTile * 4u + (unsigned)G.nt * (unsigned)sizeof(fis_trial);
+#pragma unroll
+  for (int t = 0; t < 2; ++t)
+    if (!G.direct[t])
+      b += StreamSmem::kArrays * StreamSmem::kStateWords * 4u + StreamSmem::kFlagBytes;
+  return b;
+}
+
+// Make `bar`'s current phase wait for this thread's earlier 4-byte async
+// copies (the pending count rises by one now and falls when they land).
+__device__ __forceinline__ void cp_async_arrive(uint64_t* bar) {
+  asm volatile("cp.async.mbarrier.arrive.shared::cta.b64 [%0];\n" ::"r"(smem_addr(bar))
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];\n" ::"r"(smem_addr(bar))
+               : "memory");
+}
+
+// Warp 0: all copies of item G into ring buffer `sr`, raster-word buffer
+// `sprev`, trial-record buffer `strl` and the state buffer, completing on
+// `bar`.  The raster words go first: their arrivals raise the barrier's
+// pending count before the expect-tx arrival that would otherwise let the
+// phase complete.
+__device__ __forceinline__ void stream_stage(const fis_engine& E, const int32_t* ring,
+                                             const int b0, const int nb, const int K,
+                                             const ItemGeo& G, int32_t (*sr)[kTile],
+                                             uint32_t (*sprev)[kUpdThreads / kWarp],
+                                             fis_trial* strl,
+                                             float (*sst)[StreamSmem::kArrays][StreamSmem::kStateWords],
+                                             uint8_t (*sfl)[StreamSmem::kFlagBytes],
+                                             uint64_t* bar, const int slot_prev) {
+  const int lane = threadIdx.x;
+  const int Wd = (E.n + kWarp - 1) / kWarp;
+  {
+    const int t = lane / (kUpdThreads / kWarp), w = lane % (kUpdThreads / kWarp);
+    if (t < G.nt && G.tile * kTile + w * kWarp < E.n) {
+      const int64_t word = ((int64_t)(b0 + 2 * G.pp + t) * Wd + G.tile * (kTile / kWarp) + w) *
+                               E.p.lag + slot_prev;
+      cp_async4(&sprev[t][w], E.bits + word, policy_keep());
+      cp_async_arrive(bar);
+    }
+  }
+  __syncwarp();
+  if (lane == 0) mbar_arrive_expect_tx(bar, item_bytes(G, K));
+  __syncwarp();
+  if (E.inject_stall) return;
+  const int NR = ring_row(E.n);
+  const int64_t sstride = (int64_t)((nb + 1) >> 1) * NR * 2;
+  const int64_t toff = ((int64_t)G.pp * NR + G.tile * kTile) * 2;
+  if (lane < K)
+    bulk_load(&sr[lane][0], reinterpret_cast<const uint16_t*>(ring) + (int64_t)lane * sstride + toff,
+              kTile * 4u, bar, policy_keep());
+  // the pair's trial records (consecutive), then the state rows: lane =
+  // trial * 6 + array (array 5 = the flags)
+  if (lane == 2 * (StreamSmem::kArrays + 1))
+    bulk_load(strl, E.trials + (b0 + 2 * G.pp), (unsigned)G.nt * (unsigned)sizeof(fis_trial),
+              bar, policy_keep());
+  const int t = lane / (StreamSmem::kArrays + 1), a = lane % (StreamSmem::kArrays + 1);
+  const bool direct = t == 0 ? G.direct[0] : G.direct[1];  // selected, not indexed
+  const int64_t first = t == 0 ? G.first[0] : G.first[1];
+  if (t >= 2 || direct) return;
+  const uint64_t pol = policy_stream();
+  if (a < StreamSmem::kArrays) {
+    const float* base = a == 0   ? E.v
+                        : a == 1 ? E.g
+                        : a == 2 ? E.refrac
+                        : a == 3 ? E.rates
+                                 : reinterpret_cast<const float*>(E.kicks);
+    bulk_load(&sst[t][a][0], base + (first - (first & 3)), StreamSmem::kStateWords * 4u, bar,
+              pol);
+  } else {
+    bulk_load(&sfl[t][0], E.flags + (first - (first & 15)), StreamSmem::kFlagBytes, bar, pol);
+  }
+}
+
+// Grid: up to 4 CTAs per SM, each a near-equal run of the group's items.
 __global__ void __launch_bounds__(kUpdThreads, 4)
-k_update_pair(const fis_engine E, const int b0, const int nb, const int K,
-              int32_t* __restrict__ ring, float* __restrict__ spikes_out,
-              const int bump, const float unit, const fis_clock clk, const int clk_given) {
+k_update_stream(const fis_engine E, const int b0, const int nb, const int K,
+                int32_t* __restrict__ ring, float* __restrict__ spikes_out, const int bump,
+                const float unit, const fis_clock clk, const int clk_given) {
   extern __shared__ __align__(128) uint8_t dsm[];
-  using S = PairSmem<kHalf>;
-  auto sring = reinterpret_cast<int32_t(*)[FIS_MAX_BLOCK][StagedRow<kHalf>::kWords]>(dsm);
+  using S = StreamSmem;
+  auto sring = reinterpret_cast<int32_t(*)[FIS_MAX_BLOCK][kTile]>(dsm);
+  auto sst = reinterpret_cast<float(*)[S::kArrays][S::kStateWords]>(dsm + S::kState);
+  auto sfl = reinterpret_cast<uint8_t(*)[S::kFlagBytes]>(dsm + S::kFlags);
   uint32_t* szero = reinterpret_cast<uint32_t*>(dsm + S::kZero);
   auto sbal = reinterpret_cast<uint32_t(*)[kUpdThreads / kWarp][FIS_MAX_BLOCK]>(dsm + S::kBal);
-  uint64_t* sbar = reinterpret_cast<uint64_t*>(dsm + S::kBar);
-  float* pre = reinterpret_cast<float*>(dsm + S::kPre);
+  auto sprev = reinterpret_cast<uint32_t(*)[2][kUpdThreads / kWarp]>(dsm + S::kPrev);
+  auto strl = reinterpret_cast<fis_trial(*)[2]>(dsm + S::kTrials);
+  uint64_t* full = reinterpret_cast<uint64_t*>(dsm + S::kBar);
+  uint64_t* taken = full + 2;
+  fis_clock* sck = reinterpret_cast<fis_clock*>(dsm + S::kClock);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(dsm + S::kAbort);
+
   const int n = E.n;
-  const int pp = blockIdx.y;
-  const int tile0 = blockIdx.x * 2;
-  const bool two = tile0 + 1 < ring_row(n) / kTile;
-  if (threadIdx.x < kWarp) {
-    stage_tile<kHalf>(E, ring, nb, K, pp, tile0, sring[0], &sbar[0]);
-    if (two) stage_tile<kHalf>(E, ring, nb, K, pp, tile0 + 1, sring[1], &sbar[1]);
+  const int ntiles = ring_row(n) / kTile;
+  const int items = ((nb + 1) >> 1) * ntiles;
+  const int j0 = (int)((int64_t)blockIdx.x * items / gridDim.x);
+  const int j1 = (int)((int64_t)(blockIdx.x + 1) * items / gridDim.x);
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int wib = threadIdx.x / kWarp;
+  const bool w0 = threadIdx.x < kWarp;
+  const unsigned polls = E.wait_polls ? E.wait_polls : kWaitPolls;
+  const uint64_t stream = policy_stream();
+
+  if (threadIdx.x == 0) {
+    *sck = clk_given ? clk : *E.clock;  // the block's clock
+    *abort_flag = 0;
+    mbar_init(&full[0], 1);
+    mbar_init(&full[1], 1);
+    mbar_init(taken, kUpdThreads / kWarp);
+    fence_mbar_init();
   }
-  if (two) {
-    const uint64_t stream = policy_stream();
-    const int nt = (2 * pp + 1 < nb) ? 2 : 1;
-    const int i = (tile0 + 1) * kTile + threadIdx.x;
+  if (w0) {
+#pragma unroll
+    for (int q = 0; q < kTile / kWarp; ++q) szero[q * kWarp + lane] = kEmptyPair;
+    fence_proxy_async_shared();
+  }
+  __syncthreads();
+  const fis_clock& ck = *sck;
+  const int slot_prev = ck.slot == 0 ? E.p.lag - 1 : ck.slot - 1;
+  // With `bump` the grid's last CTA advances the clock: each CTA counts
+  // itself in once every thread can read the clock from shared memory.
+  unsigned arrived = 0;
+  if (bump && threadIdx.x == 0) arrived = atomicAdd(E.done, 1u) + 1u;
+  int issued = j0 - 1, seen = j0 - 1;  // warp 0: items staged / waited for
+  if (w0 && j0 < j1) {
+    stream_stage(E, ring, b0, nb, K, item_geo(E, b0, nb, ntiles, j0), sring[0], sprev[0],
+                 strl[0], sst, sfl, &full[0], slot_prev);
+    issued = j0;
+  }
+
+  for (int j = j0; j < j1; ++j) {
+    const int s = (j - j0) & 1;
+    const unsigned par = (unsigned)((j - j0) >> 1) & 1u;
+    const ItemGeo G = item_geo(E, b0, nb, ntiles, j);
+    const int pp = G.pp, tile = G.tile, nt = G.nt;
+    const int i = tile * kTile + threadIdx.x;
+    const bool valid = i < n;
+    const bool warp_valid = (i - lane) < n;
+    int64_t sidx[2];
+#pragma unroll
+    for (int t = 0; t < 2; ++t) sidx[t] = G.first[t] + threadIdx.x;
+    // A wait that runs out ends this warp's run (decided by the whole warp,
+    // which stays together for its ballots): the error goes to the host, the
+    // other warps see the abort or run out in turn, and warp 0 drains the
+    // copies it issued before the CTA ends.
+    const bool ok = __all_sync(0xFFFFFFFFu, mbar_wait(&full[s], par, polls));
+    if (!ok) {
+      if (lane == 0) {
+        atomicOr(E.done + 1, (uint32_t)FIS_ERR_STAGE);
+        *abort_flag = 1;
+      }
+      break;
+    }
+    if (w0) seen = j;
+    fis_trial tr[2];
+#pragma unroll
+    for (int t = 0; t < 2; ++t) tr[t] = strl[s][t < nt ? t : 0];
+
+    // this item's state, from the state buffer (or directly)
+    uint32_t fl[2] = {0u, 0u}, dm[2] = {0u, 0u};
+    float rate[2] = {0.f, 0.f}, vv[2] = {0.f, 0.f}, gg[2] = {0.f, 0.f}, rr[2] = {0.f, 0.f};
+    bool bit[2];
 #pragma unroll
     for (int t = 0; t < 2; ++t) {
-      if (i < n && t < nt) {
-        const int64_t si = (int64_t)(b0 + 2 * pp + t) * n + i;
-        const void* src[5] = {E.v + si, E.g + si, E.refrac + si, E.rates + si, E.kicks + si};
-#pragma unroll
-        for (int a = 0; a < 5; ++a)
-          cp_async4(&pre[(a * 2 + t) * kUpdThreads + threadIdx.x], src[a], stream);
+      bit[t] = (sprev[s][t][wib] >> lane) & 1u;
+      if (valid && t < nt) {
+        if (!G.direct[t]) {
+          const int o = G.ofs[t] + threadIdx.x;
+          vv[t] = sst[t][0][o];
+          gg[t] = sst[t][1][o];
+          rr[t] = sst[t][2][o];
+          rate[t] = sst[t][3][o];
+          dm[t] = __float_as_uint(sst[t][4][o]);
+          fl[t] = sfl[t][G.ofb[t] + threadIdx.x];
+        } else {
+          fl[t] = ld_hint(E.flags + sidx[t], stream);
+          vv[t] = ld_hint(E.v + sidx[t], stream);
+          gg[t] = ld_hint(E.g + sidx[t], stream);
+          rr[t] = ld_hint(E.refrac + sidx[t], stream);
+          rate[t] = ld_hint(E.rates + sidx[t], stream);
+          dm[t] = ld_hint(E.kicks + sidx[t], stream);
+        }
       }
     }
-    cp_async_commit();
+    __syncwarp();
+    if (lane == 0) mbar_arrive(taken);
+
+    if (w0) {
+      if (j + 1 < j1) {
+        // every warp has taken item j's state, so has finished item j-1:
+        // stage s ^ 1, the state buffer and the small buffers s ^ 1 may be
+        // refilled
+        const bool room = __all_sync(
+            0xFFFFFFFFu, mbar_wait(taken, (unsigned)(j - j0) & 1u, polls) && !*abort_flag);
+        if (room) {
+          stream_stage(E, ring, b0, nb, K, item_geo(E, b0, nb, ntiles, j + 1), sring[s ^ 1],
+                       sprev[s ^ 1], strl[s ^ 1], sst, sfl, &full[s ^ 1], slot_prev);
+          issued = j + 1;
+        } else if (lane == 0) {
+          atomicOr(E.done + 1, (uint32_t)FIS_ERR_STAGE);
+          *abort_flag = 1;
+        }
+      }
+      // this item's slots back to empty in the ring (see update_tile)
+      const int NR = ring_row(n);
+      const int64_t sstride = (int64_t)((nb + 1) >> 1) * NR * 2;
+      const int64_t toff = ((int64_t)pp * NR + tile * kTile) * 2;
+      if (lane < K)
+        bulk_store(reinterpret_cast<uint16_t*>(ring) + (int64_t)lane * sstride + toff, szero,
+                   kTile * 4u, policy_keep());
+      bulk_commit();
+    }
+
+    TileState St;
+    bool drv_any = false;
+    const int64_t t0 = ck.step;
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      St.ka[t] = (int)max((int64_t)0, min(tr[t].start - t0, (int64_t)K));
+      St.kb[t] = (int)max((int64_t)0, min(tr[t].end - t0, (int64_t)K));
+      St.runs[t] = t < nt && St.ka[t] < St.kb[t];
+      const bool on = St.runs[t];
+      const float prob = __fmul_rn(rate[t], E.p.prob_scale);
+      St.dm[t] = (on && prob > 0.f) ? dm[t] : 0u;
+      drv_any = drv_any || (valid && on && prob > 0.f);
+      St.fl[t] = on ? fl[t] : 0u;
+      St.v[t] = on ? vv[t] : 0.f;
+      St.g[t] = on ? gg[t] : 0.f;
+      St.r[t] = on ? rr[t] : 0.f;
+      St.vclamp[t] = tr[t].v_clamp;
+      St.s_prev[t] = on && warp_valid && t0 - 1 >= tr[t].start - tr[t].history && t0 >= 1 &&
+                     bit[t];
+    }
+    const bool warp_driven = __any_sync(0xFFFFFFFFu, drv_any);
+    if (St.runs[0] || St.runs[1])
+      tile_compute<false, true>(E, b0, K, spikes_out, unit, ck, tile, pp, sring[s], sbal, St,
+                                warp_driven, sidx);
+    if (__any_sync(0xFFFFFFFFu, *abort_flag != 0)) break;
   }
-  const fis_clock ck = clk_given ? clk : *E.clock;
-  unsigned arrived = 0;
-  update_tile<false, kHalf>(E, b0, nb, K, ring, spikes_out, unit, ck, tile0, sring[0], &sbar[0],
-                            szero, sbal, nullptr, bump != 0, &arrived);
-  if (two)
-    update_tile<false, kHalf>(E, b0, nb, K, ring, spikes_out, unit, ck, tile0 + 1, sring[1],
-                              &sbar[1], szero, sbal, pre, false, &arrived);
-  clock_bump(E, bump, arrived, ck, K);
+  if (w0) {
+    // copies still in flight (a run cut short) land before the CTA ends
+    bool lost = false;
+    for (int j = seen + 1; j <= issued; ++j)
+      lost |= !__all_sync(0xFFFFFFFFu, mbar_wait(&full[(j - j0) & 1],
+                                                 (unsigned)((j - j0) >> 1) & 1u, polls));
+    cp_async_wait_all();
+    if (lost && lane == 0) atomicOr(E.done + 1, (uint32_t)FIS_ERR_STAGE_LOST);
+    // the clearing copies have read szero before the CTA ends
+    bulk_wait_all();
+  }
+  if (threadIdx.x == 0) clock_bump(E, bump, arrived, ck, K);
 }
 
 // ---------------------------------------------------------------------------
@@ -1560,21 +1866,28 @@ int update_block(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, i
   if (clk) c = *clk;
   const int given = clk ? 1 : 0;
   const int bp = bump ? 1 : 0;
-  if (!e->vstim && e->ring16 && k_steps > 1 && e->update_tiles == 2) {
-    // two tiles per CTA: the attribute for its dynamic shared memory is set
+  const auto a16 = [](const void* q) { return ((uintptr_t)q & 15u) == 0; };
+  if (!e->vstim && e->ring16 && k_steps > 1 && e->update_tiles == 2 && a16(e->v) &&
+      a16(e->g) && a16(e->refrac) && a16(e->rates) && a16(e->kicks) && a16(e->flags) &&
+      a16(e->trials)) {
+    // streamed tiles: the attributes for its dynamic shared memory are set
     // once per device
     static int sized[64] = {0};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !sized[dev]) {
-      const cudaError_t err = cudaFuncSetAttribute(
-          k_update_pair<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-          (int)PairSmem<true>::kBytes);
+      cudaError_t err = cudaFuncSetAttribute(
+          k_update_stream, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)StreamSmem::kBytes);
+      if (err == cudaSuccess)
+        err = cudaFuncSetAttribute(k_update_stream,
+                                   cudaFuncAttributePreferredSharedMemoryCarveout, 100);
       if (err != cudaSuccess) return (int)err;
       sized[dev] = 1;
     }
-    const dim3 pgrid((ring_row(e->n) / kTile + 1) / 2, (nb + 1) / 2);
-    k_update_pair<true><<<pgrid, kUpdThreads, PairSmem<true>::kBytes, st>>>(
+    // as many CTAs as fit at once (4 per SM), each a near-equal run of items
+    const int items = ((nb + 1) / 2) * (ring_row(e->n) / kTile);
+    const int grid = std::min(items, 4 * sm_count());
+    k_update_stream<<<grid, kUpdThreads, StreamSmem::kBytes, st>>>(
         *e, b0, nb, k_steps, ring, spikes_out, bp, 1.0f, c, given);
     return launch_status();
   }

@@ -211,11 +211,11 @@ class Core:
         ``drive_ctas``: scattering and drive CTAs per 8 SMs (0: the library's
         default for the mode).  ``update_streams`` 2: in the overlapped native
         loop, consecutive updates (of different trial groups) alternate
-        between two streams.  ``update_tiles`` 2: each update CTA takes two
-        256-neuron tiles and fetches the second one's input while the first
-        one's steps run (None: ``FIS_UPDATE_TILES``, else 1; two measured
-        slower on the bench: half the CTAs, and their shared memory leaves the
-        SM little L1).
+        between two streams.  ``update_tiles`` 2: streamed tiles -- up to 4
+        update CTAs per SM, each pipelining a run of (trial pair, tile) items
+        whose input arrives by bulk copies while the previous item's steps
+        run (None: ``FIS_UPDATE_TILES``, else 1; measured ~24 % slower than
+        one tile per CTA on the bench, which stays the default).
         """
         if scatter_mode is None:
             scatter_mode = int(os.environ.get("FIS_SCATTER_MODE", "1"))

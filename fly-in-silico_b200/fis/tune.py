@@ -21,8 +21,9 @@ Tunables (all exact: they change scheduling and storage, never results):
 * ``update_streams`` -- 1, or 2: consecutive updates (of different trial
   groups, so independent) alternate between two streams and overlap their
   tails.
-* ``update_tiles`` -- 256-neuron tiles per update CTA, 1 or 2 (the second
-  tile's input is fetched while the first one's steps run).
+* ``update_tiles`` -- 1 (one 256-neuron tile per update CTA) or 2 (streamed
+  tiles: each CTA pipelines a run of tiles, the next one's input fetched by
+  bulk copies while the current one's steps run).
 
 The block length stays the delay lag (20 steps), the longest that keeps the
 steps of a block independent.  The search is coordinate-wise: group x ring at

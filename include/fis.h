@@ -177,11 +177,13 @@ typedef struct fis_engine {
   int32_t update_streams;  /* fis_advance_overlap: 2 = consecutive updates
                               (of different trial groups) alternate between
                               the caller's stream and a second one; else 1 */
-  int32_t update_tiles;    /* 256-neuron tiles per update CTA: 2 = each CTA
-                              stages both tiles' slots at entry and fetches
-                              the second tile's state into shared memory
-                              while the first one's steps run (paired int16
-                              ring, Philox drive, blocks of 2+ steps); else 1 */
+  int32_t update_tiles;    /* 2 = streamed tiles: up to 4 CTAs per SM, each
+                              pipelining a run of (trial pair, tile) items --
+                              the next item's slots, state and trial records
+                              arrive by bulk copies while the current one's
+                              steps run (paired int16 ring, Philox drive,
+                              blocks of 2+ steps, arrays and trial records on
+                              16-byte boundaries); else 1 tile per CTA      */
   int32_t pad3_;
   fis_lif_params p;
 } fis_engine;

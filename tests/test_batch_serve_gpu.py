@@ -135,14 +135,16 @@ def test_overlapped_advance_equals_sequential(ring, scatter_mode, update_streams
     assert np.array_equal(got[1][0][3], oracle_trial(c, s)[1])
 
 
-def test_bounded_wait_reports_error_and_context_survives():
+@pytest.mark.parametrize("tiles", [1, 2])
+def test_bounded_wait_reports_error_and_context_survives(tiles):
     """A staging wait that runs out sets an error bit the host raises on; the
-    CUDA context stays usable and a fresh batch is exact again."""
+    CUDA context stays usable and a fresh batch is exact again (one tile per
+    update CTA, and the streamed tiles)."""
     from fis.batch import Batch
 
     c = conn()
     sp = specs(71, 2, 40)
-    b = Batch(c, 2, group=2)
+    b = Batch(c, 2, group=2, update_tiles=tiles)
     b.core.desc.wait_polls = 2000
     b.core.desc.inject_stall = 1    # no staging copy is issued: every wait runs out
     with pytest.raises(RuntimeError, match="error bits"):
