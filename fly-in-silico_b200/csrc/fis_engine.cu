@@ -1129,13 +1129,19 @@ __device__ __forceinline__ void update_tile(
   // is not used, its threshold infinite, nothing of it stored.
   fis_trial tr[2];
   int64_t sidx[2];
-  uint32_t fl[2], dm[2];
+  uint32_t fl[2], dm[2], word[2];
   float rate[2], vv[2], gg[2], rr[2];
 #pragma unroll
   for (int t = 0; t < 2; ++t) {
     const int b = b0 + 2 * pp + (t < nt ? t : 0);
     tr[t] = E.trials[b];
     sidx[t] = (int64_t)b * n + i;
+    // the warp's raster word of the step before the block: whether it is
+    // used depends on the trial record, its address does not, so it is
+    // requested now rather than after the record arrives
+    word[t] = warp_valid ? E.bits[((int64_t)b * Wd + (i >> 5)) * L +
+                                  (ck.slot == 0 ? L - 1 : ck.slot - 1)]
+                         : 0u;
     fl[t] = dm[t] = 0;
     rate[t] = vv[t] = gg[t] = rr[t] = 0.f;
     if (valid && t < nt) {
@@ -1149,10 +1155,8 @@ __device__ __forceinline__ void update_tile(
   }
   __syncthreads();  // the staging barrier exists before anyone waits on it
   const int64_t t0 = ck.step;
-  const int slot0 = ck.slot;  // ring-of-lists slot of step t0
   int ka[2], kb[2];
   bool runs[2];
-  uint32_t* bitrow[2];  // this warp's raster words, one per slot: bits[b][word][slot]
   bool s_prev[2];
   bool drv_any = false;
 #pragma unroll
@@ -1177,10 +1181,8 @@ __device__ __forceinline__ void update_tile(
       dm[t] = __fmul_rn((float)(x >> 8), 0x1p-24f) < prob ? 1u : 0u;
     }
     drv_any = drv_any || (valid && runs[t] && __fmul_rn(rate[t], E.p.prob_scale) > 0.f);
-    bitrow[t] = E.bits + ((int64_t)(b0 + 2 * pp + (t < nt ? t : 0)) * Wd + (i >> 5)) * L;
-    s_prev[t] = false;
-    if (runs[t] && warp_valid && t0 - 1 >= tr[t].start - tr[t].history && t0 >= 1)
-      s_prev[t] = (bitrow[t][slot0 == 0 ? L - 1 : slot0 - 1] >> lane) & 1u;
+    s_prev[t] = runs[t] && warp_valid && t0 - 1 >= tr[t].start - tr[t].history && t0 >= 1 &&
+                ((word[t] >> lane) & 1u);
   }
   const bool warp_driven = !kTape && __any_sync(0xFFFFFFFFu, drv_any);
 
