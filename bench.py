@@ -42,9 +42,9 @@ CONN_SEED = 0
 # Update-kernel DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum)
 # per trial-neuron and block, from one ncu capture of an 8-trial, 20-step
 # launch at steady activity with the caches kept warm, as the live pipeline
-# leaves them (82.6 MB: the scratch ring is partly served from L2).  Scaled to
+# leaves them (83.3 MB: the scratch ring is partly served from L2).  Scaled to
 # the bench's launch size by the neurons it processes.
-NCU_TRAFFIC_PER_NEURON_BLOCK = 82.59e6 / (8 * 138_639)
+NCU_TRAFFIC_PER_NEURON_BLOCK = 83.34e6 / (8 * 138_639)
 
 
 def update_bytes_per_neuron_block(core):
