@@ -373,18 +373,31 @@ __device__ __forceinline__ void scatter_body(const fis_engine& E, const ScatterA
 // Philox work is packed whatever the density of driven neurons.  The kick
 // steps of the block go to kicks[b][i] as bits (bit k = step t0 + k), written
 // for neurons with a positive rate only: the update reads them only there.
+// With the caller's lists of driven neurons (drive_idx / drive_len) a warp
+// takes 256 list entries of one trial instead of 256 neurons, so the drive
+// reads the rates of the listed neurons only; the draws are the same.
 constexpr int kDriveThreads = 256;
 constexpr int kDriveSpan = 256;  // neurons per warp task
 
 // kAllLoads: read the span's eight rate words before the first ballot (one
 // round trip per task) instead of four at a time.
+// The drive's per-warp lists in shared memory (declared once in k_phase_a,
+// shared by both forms of the drive): the driven entries of the warp's task
+// (offsets in the span), their kick probabilities and their kick bits.
+struct DriveSmem {
+  uint16_t (*slist)[kDriveSpan];
+  float (*sprob)[kDriveSpan];
+  uint32_t (*sbits)[kDriveSpan];
+};
+
 template <bool kAllLoads>
 __device__ __forceinline__ void drive_body(const fis_engine& E, const int b0, const int nb,
                                            const int K, const fis_clock& clk,
-                                           const int clk_given, const int bid, const int nblk) {
-  __shared__ uint16_t slist[kDriveThreads / kWarp][kDriveSpan];  // offset in the span
-  __shared__ float sprob[kDriveThreads / kWarp][kDriveSpan];
-  __shared__ uint32_t sbits[kDriveThreads / kWarp][kDriveSpan];
+                                           const int clk_given, const int bid, const int nblk,
+                                           const DriveSmem& sm) {
+  uint16_t (*slist)[kDriveSpan] = sm.slist;
+  float (*sprob)[kDriveSpan] = sm.sprob;
+  uint32_t (*sbits)[kDriveSpan] = sm.sbits;
   const int n = E.n;
   const int lane = threadIdx.x & (kWarp - 1);
   const int w = threadIdx.x / kWarp;
@@ -454,6 +467,117 @@ __device__ __forceinline__ void drive_body(const fis_engine& E, const int b0, co
     uint32_t* kicks = E.kicks + (int64_t)b * n + i0;
     for (int j = lane; j < cnt; j += kWarp) kicks[slist[w][j]] = sbits[w][j];
     __syncwarp();  // the lists are reused by the warp's next task
+  }
+}
+// The drive over the caller's lists of driven neurons (drive_idx /
+// drive_len).  A task is kListSpan entries of one running trial's list: all
+// of them are usually driven, so a task holds about as many draws as a
+// scan task of kDriveSpan neurons holds in a trial where a few percent of
+// the neurons are driven, and the draws spread over as many warps.
+// Every warp reads the group's trial records and list lengths itself, 32
+// trials at a time (one round trip per 32 trials), scans the trials' task
+// counts across its lanes and takes tasks gw, gw + W, ... of the group's
+// sequence, so no warp spends a round trip on a task that holds nothing.
+// Within a task: the entries' neuron indices, then their rates, each as one
+// round of loads; then the same draws as drive_body.
+__device__ __forceinline__ void drive_list_body(const fis_engine& E, const int b0, const int nb,
+                                                const int K, const fis_clock& clk,
+                                                const int clk_given, const int bid,
+                                                const int nblk, const DriveSmem& sm) {
+  constexpr unsigned kAll = 0xFFFFFFFFu;
+  constexpr int kListSpan = kWarp;  // entries per task
+  constexpr int kPer = kListSpan / kWarp;
+  const int n = E.n;
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int w = threadIdx.x / kWarp;
+  const fis_clock ck = clk_given ? clk : *E.clock;
+  const int64_t t0 = ck.step;
+  const uint64_t stream = policy_stream();
+  const int W = nblk * (kDriveThreads / kWarp);      // warps of the drive
+  const int gw = bid * (kDriveThreads / kWarp) + w;  // this warp among them
+  int acc = 0;  // tasks of the trials before this chunk of 32
+  for (int base = 0; base < nb; base += kWarp) {
+    const int bl = base + lane;
+    int nt = 0, len = 0;
+    if (bl < nb) {
+      const fis_trial t = E.trials[b0 + bl];
+      const int ka = (int)max((int64_t)0, min(t.start - t0, (int64_t)K));
+      const int kb = (int)max((int64_t)0, min(t.end - t0, (int64_t)K));
+      len = min(max(E.drive_len[b0 + bl], 0), n);
+      nt = ka < kb ? (len + kListSpan - 1) / kListSpan : 0;
+    }
+    int incl = nt;
+#pragma unroll
+    for (int off = 1; off < kWarp; off <<= 1) {
+      const int x = __shfl_up_sync(kAll, incl, off);
+      if (lane >= off) incl += x;
+    }
+    const int excl = incl - nt;
+    const int total = __shfl_sync(kAll, incl, kWarp - 1);
+    // this warp's tasks: t in [acc, acc + total) with t = gw (mod W)
+    for (int t = acc + ((gw - acc) % W + W) % W; t < acc + total; t += W) {
+      const int local = t - acc;
+      const int j = __ffs(__ballot_sync(kAll, excl <= local && local < incl)) - 1;
+      const int b = b0 + base + j;
+      const int e0 = (local - __shfl_sync(kAll, excl, j)) * kListSpan;
+      const int lenj = __shfl_sync(kAll, len, j);
+      const fis_trial tr = E.trials[b];  // read above by lane j: from L1
+      const int ka = (int)max((int64_t)0, min(tr.start - t0, (int64_t)K));
+      const int kb = (int)max((int64_t)0, min(tr.end - t0, (int64_t)K));
+      const int32_t* lst = E.drive_idx + (int64_t)b * n;
+      const float* rates = E.rates + (int64_t)b * n;
+      int ids[kPer];
+      float pr[kPer];
+#pragma unroll
+      for (int c = 0; c < kPer; ++c) {
+        const int e = e0 + c * kWarp + lane;
+        ids[c] = e < lenj ? lst[e] : -1;
+      }
+#pragma unroll
+      for (int c = 0; c < kPer; ++c)
+        pr[c] = (unsigned)ids[c] < (unsigned)n ? ld_hint(rates + ids[c], stream) : 0.f;
+      int cnt = 0;
+#pragma unroll
+      for (int c = 0; c < kPer; ++c) {
+        const float p = (unsigned)ids[c] < (unsigned)n ? __fmul_rn(pr[c], E.p.prob_scale) : 0.f;
+        const bool d = p > 0.f;
+        const unsigned m = __ballot_sync(kAll, d);
+        if (d) {
+          const int pos = cnt + __popc(m & ((1u << lane) - 1u));
+          sm.slist[w][pos] = (uint16_t)(c * kWarp + lane);
+          sm.sprob[w][pos] = p;
+          sm.sbits[w][pos] = 0u;
+        }
+        cnt += __popc(m);
+      }
+      if (cnt == 0) continue;
+      __syncwarp();
+      const int64_t own0 = t0 - tr.start;  // the trial's own step at k = 0
+      const int64_t q0 = (own0 + ka) >> 2;
+      const int nq = (int)(((own0 + kb - 1) >> 2) - q0) + 1;
+      for (int itq = lane; itq < cnt * nq; itq += kWarp) {
+        const int jd = itq / nq, qq = itq - jd * nq;
+        const int64_t quad = q0 + qq;
+        const Philox4 r4 = philox4((uint32_t)lst[e0 + sm.slist[w][jd]], (uint32_t)quad,
+                                   (uint32_t)((uint64_t)quad >> 32), tr.stream,
+                                   (uint32_t)tr.seed, (uint32_t)(tr.seed >> 32));
+        const float pj = sm.sprob[w][jd];
+        const int kq = (int)(quad * 4 - own0);  // step of word 0
+        uint32_t bits = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int k = kq + q;
+          if (k >= ka && k < kb && __fmul_rn((float)(r4.x[q] >> 8), 0x1p-24f) < pj)
+            bits |= 1u << k;
+        }
+        if (bits) atomicOr(&sm.sbits[w][jd], bits);
+      }
+      __syncwarp();
+      uint32_t* kicks = E.kicks + (int64_t)b * n;
+      for (int jj = lane; jj < cnt; jj += kWarp) kicks[lst[e0 + sm.slist[w][jj]]] = sm.sbits[w][jj];
+      __syncwarp();  // the lists are reused by the warp's next task
+    }
+    acc += total;
   }
 }
 
@@ -639,8 +763,16 @@ k_phase_a(const fis_engine E, const ScatterArgs A, const int scat) {
     else
       scatter_body(E, A, blockIdx.x, scat, pre_sum);
   } else {
-    drive_body<kMode == 1>(E, A.b0, A.nb, A.nsrc, A.clk, A.clk_given, blockIdx.x - scat,
-                           gridDim.x - scat);
+    __shared__ uint16_t slist[kDriveThreads / kWarp][kDriveSpan];
+    __shared__ float sprob[kDriveThreads / kWarp][kDriveSpan];
+    __shared__ uint32_t sbits[kDriveThreads / kWarp][kDriveSpan];
+    const DriveSmem sm{slist, sprob, sbits};
+    if (E.drive_idx)
+      drive_list_body(E, A.b0, A.nb, A.nsrc, A.clk, A.clk_given, blockIdx.x - scat,
+                      gridDim.x - scat, sm);
+    else
+      drive_body<kMode == 1>(E, A.b0, A.nb, A.nsrc, A.clk, A.clk_given, blockIdx.x - scat,
+                             gridDim.x - scat, sm);
   }
 }
 
@@ -1766,6 +1898,7 @@ int fis_check(const fis_engine* e) {
     return FIS_E_ARG;
   if (e->update_streams < 0 || e->update_streams > 2) return FIS_E_ARG;
   if (e->update_tiles < 0 || e->update_tiles > 2) return FIS_E_ARG;
+  if (!e->drive_idx != !e->drive_len) return FIS_E_ARG;  // both lists or neither
   if (!aligned16(e->edges)) return FIS_E_ALIGN;
   return FIS_OK;
 }
@@ -1837,14 +1970,17 @@ int scatter_block(const fis_engine* e, int32_t b0, int32_t nb, int32_t k_steps, 
   // drawing CTAs per SM (4.5 per SM, one wave at 5 per SM) measured best on
   // the full connectome for trial groups of 16 to 64.
   // The balanced scatter (mode 1), which keeps more loads in flight per
-  // warp, defaults to one scattering and two drawing CTAs per SM.  The
+  // warp, defaults to one scattering and two drawing CTAs per SM.  With the
+  // caller's lists of driven neurons the drive has a few percent of the
+  // rates to read, and one drawing CTA per two SMs is enough.  The
   // descriptor may set both counts (per 8 SMs, for the autotuner).
   const bool balanced = e->scatter_mode == 1;
   int drive = 0;
   if (!e->vstim && k_steps > 1) {
     const int64_t warps = (int64_t)nb * ((e->n + kDriveSpan - 1) / kDriveSpan);
-    const int64_t cap = e->drive_ctas > 0 ? std::max(1, sm_count() * e->drive_ctas / 8)
-                                          : (int64_t)sm_count() * (balanced ? 2 : 3);
+    const int64_t dflt = e->drive_idx ? std::max(1, sm_count() / 2)
+                                      : (int64_t)sm_count() * (balanced ? 2 : 3);
+    const int64_t cap = e->drive_ctas > 0 ? std::max(1, sm_count() * e->drive_ctas / 8) : dflt;
     const int64_t blocks = (warps + kDriveThreads / kWarp - 1) / (kDriveThreads / kWarp);
     drive = (int)(blocks < cap ? blocks : cap);
   }

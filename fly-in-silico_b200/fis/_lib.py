@@ -17,7 +17,7 @@ PKG = Path(__file__).resolve().parent
 LIB_NAME = "libfis_b200.so"
 LIB_PATH = PKG / LIB_NAME
 
-FIS_ABI_VERSION = 8
+FIS_ABI_VERSION = 9
 FIS_MAX_BLOCK = 20
 FIS_NOALLOC_RING_INTS = 3 << 20
 REF_EV_ABI = 3
@@ -76,6 +76,7 @@ class EngineDesc(ctypes.Structure):
                 ("list_len", ctypes.c_void_p), ("bits", ctypes.c_void_p),
                 ("clock", ctypes.c_void_p), ("done", ctypes.c_void_p),
                 ("recs", ctypes.c_void_p), ("kicks", ctypes.c_void_p),
+                ("drive_idx", ctypes.c_void_p), ("drive_len", ctypes.c_void_p),
                 ("nnz", ctypes.c_int64),
                 ("list_cap", ctypes.c_int64), ("n", ctypes.c_int32),
                 ("batch", ctypes.c_int32), ("chunk", ctypes.c_int32),

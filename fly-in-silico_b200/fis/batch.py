@@ -126,12 +126,16 @@ class Batch:
     """
 
     def __init__(self, conn: Connectome, capacity: int, params=None, device="cuda",
-                 group=None, chunk=None, core: Core | None = None, **launch):
+                 group=None, chunk=None, core: Core | None = None, drive_lists=True, **launch):
         # results come from recordings: no per-step raster needed.  `launch`:
         # the remaining Core arguments of a tuning result (ring,
-        # scatter_mode, scat_ctas, drive_ctas)
+        # scatter_mode, scat_ctas, drive_ctas).  `drive_lists`: phase A's
+        # drive visits each trial's stimulated neurons only (the batch knows
+        # them as it loads the trial) instead of scanning every rate.
         self.core = core or Core(conn, capacity, params=params, device=device, group=group,
                                  chunk=chunk, raster=False, **launch)
+        if drive_lists:
+            self.core.use_drive_lists()
         self.n = self.core.n
         self.capacity = self.core.batch
         self._copy_stream = None  # the side stream of the counts' copy to the host
@@ -221,6 +225,8 @@ class Batch:
             c.flags.view(-1)[dev[:o1].view(torch.int64)] = dev[o3:o3 + nfb]
         if nra:
             c.rates.view(-1)[dev[o1:o2].view(torch.int64)] = dev[o2:o3].view(torch.float32)
+        # the loaded trials' driven-neuron lists: the positions just written
+        c.set_drive_lists_sparse(rows, dev[o1:o2].view(torch.int64))
         for b in slots:
             if self._slot_rec[b] is not None:
                 self.release(b)

@@ -162,6 +162,9 @@ class Core:
             self.done = torch.zeros(2, dtype=torch.int32, device=dev)
             # kick steps of the current block per driven (trial, neuron)
             self.kicks = torch.zeros((B, n), dtype=torch.int32, device=dev)
+        # per-trial lists of driven neurons for phase A (use_drive_lists)
+        self.drive_idx = None
+        self.drive_len = None
         self.trials = (_lib.Trial * B)()
         for b in range(B):
             self.trials[b].start = 0
@@ -192,6 +195,8 @@ class Core:
         d.clock = self.clock.data_ptr()
         d.done = self.done.data_ptr()
         d.kicks = self.kicks.data_ptr()
+        d.drive_idx = None
+        d.drive_len = None
         d.recs = None
         d.nnz = nnz
         d.list_cap = self.list_cap
@@ -200,6 +205,58 @@ class Core:
         d.raster = 1 if self.raster else 0
         d.p = self.P
         self.set_launch(scatter_mode, scat_ctas, drive_ctas, update_streams, update_tiles)
+
+    def use_drive_lists(self):
+        """Give phase A per-trial lists of the driven neurons, so that its
+        Poisson drive reads the rates of those neurons only instead of every
+        rate (the draws and the results are the same).
+
+        From then on every write of ``rates`` must keep the lists in step:
+        each trial's first ``drive_len[b]`` entries of ``drive_idx[b]`` are a
+        superset of its neurons with a positive rate.  ``fis.batch.Batch``
+        does this as it loads trials; a caller that writes ``rates`` itself
+        calls ``rebuild_drive_lists`` afterwards.  The lists are built now
+        from the current rates.
+        """
+        if self.drive_idx is None:
+            self.drive_idx = torch.zeros((self.batch, self.n), dtype=torch.int32,
+                                         device=self.device)
+            self.drive_len = torch.zeros(self.batch, dtype=torch.int32, device=self.device)
+            self.desc.drive_idx = self.drive_idx.data_ptr()
+            self.desc.drive_len = self.drive_len.data_ptr()
+        self.rebuild_drive_lists()
+
+    def rebuild_drive_lists(self, rows=None):
+        """Rebuild the driven-neuron lists of ``rows`` (all trials by
+        default) from ``rates``: the neurons with a positive rate, ascending."""
+        if self.drive_idx is None:
+            return
+        rows = slice(None) if rows is None else rows
+        driven = self.rates[rows] > 0
+        # a stable sort of "not driven" puts each row's driven neurons first,
+        # in ascending order
+        order = torch.sort((~driven).to(torch.int8), dim=1, stable=True).indices
+        self.drive_idx[rows] = order.to(torch.int32)
+        self.drive_len[rows] = driven.sum(dim=1, dtype=torch.int32)
+
+    def set_drive_lists_sparse(self, rows, positions):
+        """Set the lists of the trials in ``rows`` (a slice or an index
+        tensor) from ``positions``: the flat positions slot * N + neuron
+        (int64, on the device, unique) of every neuron of those trials that
+        may have a positive rate."""
+        if self.drive_idx is None:
+            return
+        n = self.n
+        self.drive_len[rows] = 0
+        if positions.numel() == 0:
+            return
+        p = torch.sort(positions).values
+        slot = p // n
+        cnt = torch.bincount(slot, minlength=self.batch)
+        first = torch.cumsum(cnt, 0) - cnt
+        rank = torch.arange(p.numel(), device=p.device) - first[slot]
+        self.drive_idx[slot, rank] = (p - slot * n).to(torch.int32)
+        self.drive_len[rows] = cnt.to(torch.int32)[rows]
 
     def set_launch(self, scatter_mode=None, scat_ctas=0, drive_ctas=0, update_streams=1,
                    update_tiles=None):

@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define FIS_ABI_VERSION 8
+#define FIS_ABI_VERSION 9
 
 /* Largest number of steps one block may advance (registers per thread). */
 #define FIS_MAX_BLOCK 20
@@ -131,6 +131,16 @@ typedef struct fis_trial {
  *   kicks    uint32 [B][N]     scratch: the Poisson kick steps of the current
  *                              block, written by phase A for neurons with a
  *                              positive rate (others are never read)
+ *   drive_idx int32 [B][N] or NULL, drive_len int32 [B]: per trial b, the
+ *                              first drive_len[b] entries of row b list a
+ *                              superset of the neurons whose rate is
+ *                              positive (any order, each below N).  When
+ *                              set, phase A's Poisson drive visits only the
+ *                              listed neurons instead of scanning every
+ *                              rate; the draws and kicks are the same.  A
+ *                              neuron with a positive rate that is missing
+ *                              from its trial's list gets stale kicks: the
+ *                              caller keeps the lists in step with `rates`.
  */
 typedef struct fis_engine {
   const int64_t* row_ptr;
@@ -150,6 +160,8 @@ typedef struct fis_engine {
   uint32_t* done;
   int32_t* const* recs;
   uint32_t* kicks;
+  const int32_t* drive_idx;
+  const int32_t* drive_len;
   int64_t nnz;
   int64_t list_cap;
   int32_t n;

@@ -234,3 +234,36 @@ def test_run_many_raises_a_batch_error_when_its_counts_are_due():
     fresh = Batch(c, 2, group=2).run(sp)
     for j, s in enumerate(sp):
         assert np.array_equal(fresh[j], oracle_trial(c, s)[1]), j
+
+
+@pytest.mark.parametrize("group", [3, 8])
+def test_drive_lists_equal_the_full_scan(group):
+    """Phase A's drive over each trial's list of stimulated neurons (what
+    Batch gives it) draws exactly what the scan over every rate draws: the
+    same counts and the same final state, trial for trial, in a mix of
+    uneven durations whose trials are reloaded into freed slots."""
+    from fis.batch import Batch
+
+    c = conn()
+    first = specs(91, 7, (60, 140))
+    second = specs(92, 3, (50, 90))
+    got = []
+    for lists in (False, True):
+        b = Batch(c, 7, group=group, drive_lists=lists)
+        counts = [b.run(first), b.run(second)]
+        core = b.core
+        got.append((counts, core.v.cpu().numpy(), core.g.cpu().numpy(),
+                    core.refrac.cpu().numpy()))
+        if lists:
+            # the lists hold the stimulated neurons of the last load
+            for j, s in enumerate(second):
+                slot = b.slots_of_run[j]
+                k = int(core.drive_len[slot])
+                assert sorted(core.drive_idx[slot, :k].tolist()) == sorted(set(int(x) for x in s.stim))
+    (ca, va, ga, ra), (cb, vb, gb, rb) = got
+    for x, y in zip(ca, cb):
+        for u, w in zip(x, y):
+            assert np.array_equal(u, w)
+    assert np.array_equal(va, vb) and np.array_equal(ga, gb) and np.array_equal(ra, rb)
+    for j, s in enumerate(second):
+        assert np.array_equal(cb[1][j], oracle_trial(c, s)[1]), j

@@ -263,3 +263,48 @@ def test_result_save_load_round_trip(tmp_path):
     tl = res.region_timeline()
     want = bins[:, ::2].mean(1) / (0.01 * 2)
     assert np.allclose(tl.loc["AL"].to_numpy(), want)
+
+
+def test_drive_lists_from_rates_and_from_sparse_positions():
+    """The driven-neuron lists phase A reads (Core.use_drive_lists): rebuilt
+    from the rates, or set from the sparse positions a batch load writes,
+    each trial's first drive_len entries are its neurons with a positive
+    rate (ascending) and other trials' lists are untouched."""
+    import types
+
+    import torch
+
+    from fis.engine import Core
+
+    rng = np.random.default_rng(3)
+    B, n = 5, 97
+    rates = torch.zeros((B, n), dtype=torch.float32)
+    for b in range(B):
+        idx = rng.choice(n, size=int(rng.integers(0, 20)), replace=False)
+        rates[b, torch.as_tensor(idx)] = torch.as_tensor(rng.uniform(50, 300, idx.size),
+                                                         dtype=torch.float32)
+    fake = types.SimpleNamespace(n=n, batch=B, rates=rates,
+                                 drive_idx=torch.full((B, n), -1, dtype=torch.int32),
+                                 drive_len=torch.full((B,), -1, dtype=torch.int32))
+    Core.rebuild_drive_lists(fake)
+    for b in range(B):
+        want = torch.nonzero(rates[b] > 0).flatten().tolist()
+        k = int(fake.drive_len[b])
+        assert fake.drive_idx[b, :k].tolist() == want
+    # a load of rows 1 and 3 (positions unsorted, as packed per trial)
+    before = fake.drive_idx.clone(), fake.drive_len.clone()
+    pos = []
+    for b in (3, 1):
+        pos += [b * n + int(i) for i in rng.permutation(rng.choice(n, size=7, replace=False))]
+    rows = torch.as_tensor([1, 3])
+    Core.set_drive_lists_sparse(fake, rows, torch.as_tensor(pos, dtype=torch.int64))
+    for b in range(B):
+        k = int(fake.drive_len[b])
+        if b in (1, 3):
+            want = sorted(p - b * n for p in pos if p // n == b)
+            assert fake.drive_idx[b, :k].tolist() == want
+        else:
+            assert k == int(before[1][b])
+            assert torch.equal(fake.drive_idx[b], before[0][b])
+    Core.set_drive_lists_sparse(fake, slice(0, 2), torch.zeros(0, dtype=torch.int64))
+    assert fake.drive_len[:2].tolist() == [0, 0]
