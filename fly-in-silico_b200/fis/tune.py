@@ -28,8 +28,10 @@ Tunables (all exact: they change scheduling and storage, never results):
 The block length stays the delay lag (20 steps), the longest that keeps the
 steps of a block independent.  The search is coordinate-wise: group x ring at
 the default launch, then scatter mode x chunk at the best of those, then the
-phase-A grid, then the update streams and tiles per CTA.  Each candidate runs a short seeded trial mix on a scratch
-engine and is timed with CUDA events; the winner is stored in a JSON cache
+phase-A grid, then the update streams, then the update form (one tile per
+CTA or streamed tiles).  Each candidate runs a short seeded trial mix (the
+caller's own trials when given) on a scratch engine and is timed with CUDA
+events; the winner is stored in a JSON cache
 (``FIS_TUNE_CACHE`` or ``~/.cache/fis/tune.json``).
 """
 
@@ -56,7 +58,7 @@ def cache_path() -> Path:
 
 def _key(conn: Connectome, batch: int) -> str:
     name = torch.cuda.get_device_name() if torch.cuda.is_available() else "cpu"
-    return "%s|n=%d|e=%d|b=%d|v5" % (name, conn.n, conn.nnz, batch)
+    return "%s|n=%d|e=%d|b=%d|v6" % (name, conn.n, conn.nnz, batch)
 
 
 def load_cache() -> dict:
@@ -193,7 +195,7 @@ def tune(conn: Connectome, batch: int, params=None, groups=None, rings=None, mod
             if not seen(cand):
                 trial(cand)
     best = best_so_far()
-    # 5. one or two tiles per update CTA
+    # 5. one tile per update CTA, or the streamed tiles
     for tiles in (1, 2):
         cand = dict(best, update_tiles=tiles)
         if not seen(cand):
