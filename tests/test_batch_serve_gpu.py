@@ -267,3 +267,24 @@ def test_drive_lists_equal_the_full_scan(group):
     assert np.array_equal(va, vb) and np.array_equal(ga, gb) and np.array_equal(ra, rb)
     for j, s in enumerate(second):
         assert np.array_equal(cb[1][j], oracle_trial(c, s)[1]), j
+
+
+def test_tuner_runoff_and_tuned_launch_is_exact():
+    """The autotuner on a small connectome: it times its candidates, runs the
+    fastest three again (the runoff that picks the winner), and the launch it
+    returns gives the same counts as the oracle, trial for trial."""
+    from fis.batch import Batch
+    from fis.tune import core_kwargs, tune
+
+    c = conn()
+    sp = specs(95, 8, 60)
+    best = tune(c, 8, groups=[2, 4, 8], chunks=[256], grids=[(8, 8)], steps=40, reps=1,
+                use_cache=False, specs=sp, tag="test")
+    cands = best["candidates"]
+    assert len(cands) >= 3
+    ran = [r for r in cands if "runoff_ms_per_step" in r]
+    assert len(ran) == 3
+    assert best["runoff_ms_per_step"] == min(r["runoff_ms_per_step"] for r in ran)
+    got = Batch(c, 8, **core_kwargs(best)).run(sp)
+    for j, s in enumerate(sp):
+        assert np.array_equal(got[j], oracle_trial(c, s)[1]), j
