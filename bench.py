@@ -594,10 +594,14 @@ def main():
                        "autotune_candidates": len(best["candidates"]),
                        "update_streams": core.update_streams,
                        "update_tiles": core.update_tiles,
+                       # per candidate: its launch, us per step, and (the three
+                       # fastest) us per step in the longer runoff that decides
                        "autotune": [[c[k] for k in ("group", "ring", "scatter_mode", "chunk",
                                                     "scat_ctas", "drive_ctas",
                                                     "update_streams", "update_tiles")]
                                     + [round(c["ms_per_step"] * 1000.0, 2)]
+                                    + ([round(c["runoff_ms_per_step"] * 1000.0, 2)]
+                                       if "runoff_ms_per_step" in c else [])
                                     for c in best["candidates"]],
                        "block_steps": core.max_block,
                        "l2": "inputs larger than L2 (trial state 150 MB, spike lists "
